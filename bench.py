@@ -1,0 +1,315 @@
+"""Benchmark of the nhswps time step on B200: member-steps/s at ng=256, nz=16.
+
+Workload: the single-run configuration, ng=256 horizontal, nz=16 layers (17
+levels), starting from the vstrip PV strip with a seeded N(0, 1e-3) perturbation
+of q per grid point (delta = gamma = 0); one step = one predictor-corrector
+``advance`` (main_invert + psolve + source, three times).  Synthetic data: there
+is no dataset.  All fields (>= 8.9 MB each, ~0.5 GB working set) exceed the
+126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   (CPU FP64 oracle on the host cores)
+
+Multi-GPU (torchrun): one independent member per rank (replicas, weak scaling);
+the only collectives are the timing barrier and the max-over-ranks reduction.
+"""
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "shallow-water_b200")
+NG, NZ = 256, 16
+METRIC = "member-steps/s at ng=256 nz=16"
+UNIT = "member-steps/s"
+
+
+def load_package():
+    if "shallow_water_b200" in sys.modules:
+        return sys.modules["shallow_water_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "shallow_water_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["shallow_water_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def initial_fields(ng, nz, seed, vstrip_fn):
+    """vstrip PV strip replicated over the levels + N(0, 1e-3) (seeded); delta = gamma = 0."""
+    qq2 = vstrip_fn(ng)
+    rng = np.random.default_rng(seed)
+    q3 = np.tile(qq2, nz + 1) + rng.normal(0.0, 1.0e-3, size=ng * ng * (nz + 1))
+    z3 = np.zeros_like(q3)
+    return q3, z3, z3.copy()
+
+
+def algorithmic_bytes_per_step(ng, nz, sweeps, w_fft):
+    """Algorithmic bytes of one advance step (member): one plane read + one plane
+    write per 2-D transform of the reference's decomposition, plus the float64
+    Thomas traffic per pressure sweep.  sweeps = total psolve sweeps of the step."""
+    n2 = ng * ng
+    ffts = 3 * (63 * nz + 47) + sweeps * (7 * nz + 1)
+    return ffts * 2 * n2 * w_fft + sweeps * (4 * nz + 2) * n2 * 8
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._th = threading.Thread(target=self._run, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._th.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def oracle_sample(steps, threads=None):
+    """Time `steps` oracle advance steps at ng=256, nz=16 on the host cores."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+    if threads:
+        orc.set_num_threads(threads)
+    q3, d3, g3 = initial_fields(NG, NZ, 1, orc.vstrip)
+    sp, st = orc.initial_state(NG, NZ, q3, d3, g3)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        status, _, _ = orc.advance(sp, st, ggen=True)
+        if status:
+            raise RuntimeError("oracle advance failed: %d" % status)
+    dt = time.perf_counter() - t0
+    return steps / dt, orc.num_threads(), dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, 2))
+    rate, cores, dt = oracle_sample(steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "nhswps advance, ng=256 nz=16, vstrip + N(0,1e-3) q, delta=gamma=0",
+                   "ng": NG, "nz": NZ, "members": 1},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": "%d advance step(s) of the FP64 C restatement of the reference "
+                                   "(the Rust reference cannot be built here: no cargo), OpenMP over levels" % steps},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    sw = load_package()
+    L = sw._native.lib()
+    prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
+    w_fft = 8 if prec == sw.SW_FP64 else 4
+
+    sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+    q3, d3, g3 = initial_fields(NG, NZ, 1 + rank, sw.vstrip.pv_strip)
+    st = sw.nhswps.initial_state(sp, q3, d3, g3)
+    stream_ptr = ctypes.c_void_p()
+    sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- warm-up ---------------------------------------------------------------
+    for _ in range(args.warmup):
+        sw._native.check(L.sw_advance(sp.ctx, 1, 1))
+    sw.nhswps.diag_history(sp)
+    sweeps_seen = []
+
+    # ---- device-resident timed region ------------------------------------------------
+    n0 = ctypes.c_longlong()
+    n1 = ctypes.c_longlong()
+    barrier()
+    torch.cuda.synchronize()
+    sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n0)))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            sw._native.check(L.sw_advance(sp.ctx, 1, 1))
+            sweeps_seen.append(sum(sw.nhswps.last_sweeps(sp)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n1)))
+    ms = e0.elapsed_time(e1)
+    t_local = ms / 1e3
+    if world > 1:
+        t = torch.tensor([t_local], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    else:
+        t_max = t_local
+    value = world * args.steps / t_max
+    launches = int(n1.value - n0.value)
+
+    # ---- end-to-end through the C ABI with host buffers ---------------------------------
+    n3 = sp.n3
+    pinned = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
+    outs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs")}
+    for k in pinned:
+        pinned[k].numpy()[:] = st.get(k).ravel(order="F")
+    fidx = sw._native.FIELD_INDEX
+    e2e_steps = max(2, min(args.steps, 5))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for k, buf in pinned.items():
+            sw._native.check(L.sw_state_set(sp.ctx, fidx[k], 0, ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
+        sw._native.check(L.sw_advance(sp.ctx, 1, 1))
+        for k, buf in outs.items():
+            sw._native.check(L.sw_state_get(sp.ctx, fidx[k], 0, ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
+    torch.cuda.synchronize()
+    e2e_local = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_local], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_local = float(t.item())
+    e2e_value = world * e2e_steps / e2e_local
+
+    # ---- dominant kernel: batched 2-D transform pass, timed live ---------------------
+    peak, peak_kind = measured_peak()
+    planes = 6 * (NZ + 1)
+    fbuf = torch.randn(planes * NG * NG, dtype=torch.float64 if w_fft == 8 else torch.float32, device="cuda")
+    obuf = torch.empty_like(fbuf)
+    torch.cuda.synchronize()
+    reps = 20
+    for _ in range(3):
+        sw._native.check(L.sw_fft2d_dev(sp.ctx, 0, planes, ctypes.c_void_p(fbuf.data_ptr()), ctypes.c_void_p(obuf.data_ptr())))
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for r in range(reps):
+        d = r & 1
+        src, dst = (fbuf, obuf) if d == 0 else (obuf, fbuf)
+        sw._native.check(L.sw_fft2d_dev(sp.ctx, d, planes, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
+    k1.record(stream)
+    torch.cuda.synchronize()
+    per_launch_s = k0.elapsed_time(k1) / 1e3 / (2 * reps)
+    bytes_per_launch = 2 * planes * NG * NG * w_fft
+    achieved = bytes_per_launch / per_launch_s / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "fft_pass_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get("bytes_per_launch_%s" % args.precision)
+
+    step_bytes = algorithmic_bytes_per_step(NG, NZ, float(np.mean(sweeps_seen)), w_fft)
+    step_gbs = step_bytes * (args.steps / t_local) / 1e9
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, dt = oracle_sample(1)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "1 advance step at ng=256 nz=16 of the FP64 C restatement (OpenMP over levels); %.1f s" % dt}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if w_fft == 8 else "f32+f64", "data": "synthetic",
+            "config": {"workload": "nhswps advance, ng=256 nz=16, vstrip + N(0,1e-3) q, delta=gamma=0",
+                       "ng": NG, "nz": NZ, "members_per_gpu": 1, "precision": args.precision,
+                       "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
+                       "psolve_sweeps_per_step": float(np.mean(sweeps_seen))},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * n3 * 8,
+                    "d2h_bytes_per_step": 3 * n3 * 8, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "k_fft_pass (batched 2-D transform pass, %d planes)" % planes,
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "step_algorithmic_gbs": step_gbs, "step_frac": step_gbs / peak},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

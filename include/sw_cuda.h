@@ -1,0 +1,147 @@
+/*
+ * sw_cuda.h -- C ABI of the B200 (sm_100a) implementation of the nhswps
+ * time-step path of rse-standrewscs/shallow-water.
+ *
+ * Plain C: int status codes, plain pointers and sizes, no C++ or torch types.
+ * All arrays are float64 in the reference's Fortran order (src/utils.rs:6-32):
+ *   physical plane rvar(ny,nx) -> p[iy + ng*ix], spectral svar(nx,ny) -> s[kx + ng*ky],
+ *   3-D fields add + ng*ng*iz for the nz+1 levels iz = 0..nz.
+ * Host-pointer entry points copy in and out around the GPU work; the
+ * `_dev` entry points take device pointers and a cudaStream_t (as void*).
+ * A context is not thread-safe: use one context per host thread/stream.
+ * Every entry point returns SW_OK or an error status; sw_last_error() gives the
+ * message of the calling thread's last failure.
+ */
+#ifndef SW_CUDA_H
+#define SW_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define SW_OK 0
+#define SW_ERR_FACTORISE 1       /* n not of the form 2^a 3^b 5^c (stafft/mod.rs:148-149) */
+#define SW_ERR_CUDA 2            /* CUDA runtime failure */
+#define SW_ERR_PSOLVE_DIVERGED 3 /* pressure error > 1 after a sweep (psolve.rs:349-352) */
+#define SW_ERR_PSOLVE_MAXITER 4  /* pressure iteration hit its cap (psolve.rs:360-366) */
+#define SW_ERR_ARG 6             /* invalid argument or size */
+#define SW_ERR_STATE 7           /* call made in the wrong state */
+
+/* ---- precision of the hot path ---------------------------------------------- */
+#define SW_FP64 0  /* everything in float64 */
+#define SW_MIXED 1 /* float32 FFTs/products, float64 tridiagonal solve, residual, diagnostics, time update */
+
+/* ---- fields of nhswps::State (src/nhswps/mod.rs:87-148) ------------------------ */
+enum sw_field {
+    SW_U = 0, SW_V, SW_W, SW_Z, SW_ZX, SW_ZY, SW_R, SW_RI, SW_AA, SW_ZETA,
+    SW_PN, SW_DPN, SW_PS, SW_QS, SW_DS, SW_GS, SW_NFIELDS
+};
+
+typedef struct sw_ctx sw_ctx;
+
+const char* sw_last_error(void);
+int sw_version(void);
+
+/* ---- stafft (src/stafft/mod.rs) ----------------------------------------------- */
+/* Replaces stafft::factorisen (src/stafft/mod.rs:97-150). */
+int sw_factorisen(int n, int factors[5]);
+/* Replaces stafft::initfft (src/stafft/mod.rs:67-95): trig has 2n entries. */
+int sw_initfft(int n, int factors[5], double* trig);
+/* Replace stafft::forfft / revfft (src/stafft/mod.rs:158, 301): m transforms of
+ * length n on x[i + m*j] (host memory, in place).  trig/factors are checked for
+ * consistency with n when non-NULL; the GPU keeps its own twiddle tables. */
+int sw_forfft(int m, int n, double* x, const double* trig, const int factors[5]);
+int sw_revfft(int m, int n, double* x, const double* trig, const int factors[5]);
+/* Same on device memory: precision SW_FP64 (x is double*) or SW_MIXED (x is float*). */
+int sw_forfft_dev(int m, int n, void* x, int precision, void* stream);
+int sw_revfft_dev(int m, int n, void* x, int precision, void* stream);
+
+/* ---- context: one ensemble of nmembers runs of the same (ng, nz) -------------- */
+/* Replaces Spectral::new(ng, nz) (src/spectral/mod.rs:65-299) plus the State
+ * allocation of nhswps (src/nhswps/mod.rs:190-235). */
+int sw_ctx_create(int ng, int nz, int nmembers, int precision, int device, sw_ctx** out);
+void sw_ctx_destroy(sw_ctx* ctx);
+int sw_ctx_info(const sw_ctx* ctx, int* ng, int* nz, int* nmembers, int* precision);
+/* Copy a named Spectral operator out ("hlap", "filt", "htdv", ... "kmag"); n = element count. */
+int sw_spectral_get(sw_ctx* ctx, const char* name, double* out, size_t n);
+
+/* State fields, host float64, ng*ng*(nz+1) values per member. */
+int sw_state_set(sw_ctx* ctx, int field, int member, const double* host, size_t n);
+int sw_state_get(sw_ctx* ctx, int field, int member, double* host, size_t n);
+/* Whole-ensemble copies: host holds nmembers*ng*ng*(nz+1) values, member-major. */
+int sw_state_set_all(sw_ctx* ctx, int field, const double* host, size_t n);
+int sw_state_get_all(sw_ctx* ctx, int field, double* host, size_t n);
+int sw_set_time(sw_ctx* ctx, double t);
+int sw_get_time(const sw_ctx* ctx, double* t);
+
+/* ---- spectral operators on host arrays (member-independent) ------------------- */
+/* D2FFT::ptospc / spctop (src/sta2dfft.rs:91-123): one ng*ng plane. */
+int sw_ptospc(sw_ctx* ctx, const double* rvar, double* svar);
+int sw_spctop(sw_ctx* ctx, const double* svar, double* rvar);
+/* D2FFT::xderiv / yderiv (src/sta2dfft.rs:128-184) */
+int sw_xderiv(sw_ctx* ctx, const double* var, double* der);
+int sw_yderiv(sw_ctx* ctx, const double* var, double* der);
+/* Spectral::jacob / divs (src/spectral/mod.rs:423-475): physical aa, bb -> spectral cs. */
+int sw_jacob(sw_ctx* ctx, const double* aa, const double* bb, double* cs);
+int sw_divs(sw_ctx* ctx, const double* aa, const double* bb, double* cs);
+/* Spectral::deal2d (one plane) and deal3d (nz+1 planes), in place. */
+int sw_deal2d(sw_ctx* ctx, double* fp);
+int sw_deal3d(sw_ctx* ctx, double* fp);
+/* Spectral::ptospc3d / spctop3d (src/spectral/mod.rs:479-522), levels izbeg..izend. */
+int sw_ptospc3d(sw_ctx* ctx, const double* fp, double* fs, int izbeg, int izend);
+int sw_spctop3d(sw_ctx* ctx, const double* fs, double* fp, int izbeg, int izend);
+/* Spectral::spec1d (src/spectral/mod.rs:558-591): spec has ng+1 entries. */
+int sw_spec1d(sw_ctx* ctx, const double* ss, double* spec);
+
+/* ---- nhswps numerics on the context's state (all members) ----------------------- */
+/* Spectral::main_invert (src/spectral/mod.rs:305-417): qs,ds,gs -> r,u,v,zeta. */
+int sw_main_invert(sw_ctx* ctx);
+/* vertical (src/nhswps/vertical.rs:8-143): r,u,v,ds -> z,zx,zy,aa,w. */
+int sw_vertical(sw_ctx* ctx);
+/* coeffs (src/nhswps/coeffs.rs:8-101); outputs of member 0 copied to host when non-NULL. */
+int sw_coeffs(sw_ctx* ctx, double* sigx, double* sigy, double* cpt1, double* cpt2);
+/* cpsource (src/nhswps/cpsource.rs:13-261); sp0 of member 0 to host when non-NULL. */
+int sw_cpsource(sw_ctx* ctx, double* sp0);
+/* psolve (src/nhswps/psolve.rs:16-411).  iters/errp (may be NULL) receive member
+ * 0's sweep count and final relative change.  nitmax <= 0 selects the reference's 100. */
+int sw_psolve(sw_ctx* ctx, int nitmax, int* iters, double* errp);
+/* source (src/nhswps/source.rs:19-138); outputs of member 0 to host when non-NULL. */
+int sw_source(sw_ctx* ctx, double* sqs, double* sds, double* sgs);
+/* advance (src/nhswps/advance.rs:13-279): nsteps predictor-corrector steps.
+ * ggen != 0 runs main_invert + psolve at the start of the first step (the
+ * reference's State::ggen); later steps always do. */
+int sw_advance(sw_ctx* ctx, int nsteps, int ggen);
+/* diagnose (src/nhswps/mod.rs:666-711) of one member:
+ * out = {0.5*zrms^2, zrms, zmax, umax}. */
+int sw_diagnose(sw_ctx* ctx, int member, double out[4]);
+/* Diagnostics recorded at the start of each advance step since the last call:
+ * out holds up to cap rows of {member-0 values x4}; *count gets the row count. */
+int sw_diag_history(sw_ctx* ctx, double* out, int cap, int* count);
+/* Energies of savegrid (src/nhswps/mod.rs:365-410) of one member: {ekin, epot, etot}. */
+int sw_energy(sw_ctx* ctx, int member, double out[3]);
+/* psolve sweep counts of the last advance step for member 0 (3 entries). */
+int sw_last_sweeps(sw_ctx* ctx, int out[3]);
+/* Synchronise the context's stream. */
+int sw_sync(sw_ctx* ctx);
+
+/* ---- device-resident access for benchmarking and zero-copy callers ----------------- */
+/* Device pointer of a state field (all members, member-major) and its element size
+ * in bytes (8 for the float64 fields; 4 for float32 fields of SW_MIXED). */
+int sw_field_device_ptr(sw_ctx* ctx, int field, void** ptr, int* elem_bytes);
+/* The context's CUDA stream (cudaStream_t as void*). */
+int sw_stream(sw_ctx* ctx, void** stream);
+/* Batched 2-D transforms on device memory with the context's plan: direction 0 =
+ * ptospc (physical -> spectral), 1 = spctop; nplanes ng*ng planes of the context's
+ * work precision (double for SW_FP64, float for SW_MIXED); in and out may alias.
+ * Launches two tile passes per call (reference D2FFT::ptospc/spctop, src/sta2dfft.rs:91-123). */
+int sw_fft2d_dev(sw_ctx* ctx, int direction, int nplanes, const void* in, void* out);
+/* Number of kernels the library launched on this context so far. */
+int sw_kernel_launches(sw_ctx* ctx, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,156 @@
+// Batched 2-D transforms (D2FFT::ptospc / spctop, reference src/sta2dfft.rs:91-123)
+// as two coalesced tile passes through an L2-resident intermediate.
+//
+// Layouts: physical P[iy + ng*ix], spectral S[kx + ng*ky], intermediate
+// M[iy + ng*kx] (the reference's transposed work array).
+//   spctop: pass A  reverse along ky for tiles of kx columns  (S -> M)
+//           pass B  reverse along kx for tiles of iy columns  (M -> P)
+//   ptospc: pass A  forward along ix for tiles of iy columns  (P -> M)
+//           pass B  forward along iy for tiles of kx columns  (M -> S)
+// User functors:
+//   spctop: ld(o, kx, ky) -> T spectral input,  st(o, iy, ix, T) physical output
+//   ptospc: ld(o, iy, ix) -> T physical input,  st(o, kx, ky, T) spectral output
+// so products, derivatives, filters and combinations fuse into the passes.
+#pragma once
+#include "sw_core.cuh"
+
+namespace sw {
+
+template <class LD>
+struct LdOff {
+    LD f;
+    int o0;
+    __device__ __forceinline__ auto operator()(int o, int c, int p) const { return f(o0 + o, c, p); }
+};
+template <class ST>
+struct StOff {
+    ST f;
+    int o0;
+    template <class V>
+    __device__ __forceinline__ void operator()(int o, int c, int p, V v) const { f(o0 + o, c, p, v); }
+};
+// intermediate addressed [pt + ng*col] (point index contiguous)
+template <typename T>
+struct MidPC {
+    T* m;
+    int ng;
+    __device__ __forceinline__ T operator()(int o, int c, int p) const { return m[((size_t)o * ng + c) * ng + p]; }
+    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { m[((size_t)o * ng + c) * ng + p] = v; }
+};
+// intermediate addressed [col + ng*pt] (column index contiguous)
+template <typename T>
+struct MidCP {
+    T* m;
+    int ng;
+    __device__ __forceinline__ T operator()(int o, int c, int p) const { return m[((size_t)o * ng + p) * ng + c]; }
+    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { m[((size_t)o * ng + p) * ng + c] = v; }
+};
+
+inline int build_plan(int n, FftPlan& plan) {
+    int rem = n;
+    plan.n = n;
+    plan.nrad = 0;
+    if (n < 2) return SW_ERR_FACTORISE;
+    const int order[4] = {4, 2, 3, 5};
+    for (int r : order)
+        while (rem % r == 0) {
+            if (plan.nrad >= FFT_MAX_RAD) return SW_ERR_FACTORISE;
+            plan.rad[plan.nrad++] = r;
+            rem /= r;
+        }
+    return rem == 1 ? SW_OK : SW_ERR_FACTORISE;
+}
+
+// Twiddles exp(-2 pi i t/n), t < n, computed in float64 on the host.
+template <typename T>
+inline std::vector<typename C2<T>::t> host_twiddles(int n) {
+    std::vector<typename C2<T>::t> tw(n);
+    for (int t = 0; t < n; t++) {
+        const double a = 2.0 * PI * (double)t / (double)n;
+        tw[t].x = (T)std::cos(a);
+        tw[t].y = (T)(-std::sin(a));
+    }
+    return tw;
+}
+
+// Columns per CTA: even, keeps the pass within ~72 KB of shared memory.
+template <typename T>
+inline int pick_tile(int n) {
+    const int budget = 72 * 1024 / (int)sizeof(typename C2<T>::t);
+    int tc = budget / n - 1;
+    if (tc > 32) tc = 32;
+    tc &= ~1;
+    if (tc < 2) tc = 2;
+    return tc;
+}
+
+template <typename T, bool INV, bool LCF, bool SCF, class LD, class ST>
+inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T>::t* tw, int tc, T sc,
+                        int nout, int ncols, LD ld, ST st) {
+    if (nout <= 0) return;
+    auto kern = k_fft_pass<T, INV, LCF, SCF, LD, ST>;
+    const size_t smem = fft_pass_smem<T>(plan.n, tc);
+    static int attr_done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !attr_done[dev]) {
+        SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_done[dev] = 1;
+    }
+    dim3 grid((ncols + tc - 1) / tc, nout);
+    kern<<<grid, FFT_THREADS, smem, s>>>(plan, tw, ncols, tc, sc, ld, st);
+    SW_CHECK_LAUNCH();
+    count_launch();
+}
+
+template <typename T>
+struct Fft2d {
+    using T2 = typename C2<T>::t;
+    int ng = 0;
+    FftPlan plan{};
+    DevBuf<T2> tw;
+    DevBuf<T> mid;
+    int cap = 0;  // planes the intermediate holds
+    int tc = 2;
+    T sc = 1;
+
+    void init(int ng_, int cap_planes) {
+        ng = ng_;
+        require(build_plan(ng, plan) == SW_OK, SW_ERR_FACTORISE, "grid size must factor into 2, 3, 5");
+        auto h = host_twiddles<T>(ng);
+        tw.alloc(ng);
+        SW_CUDA(cudaMemcpy(tw.p, h.data(), sizeof(T2) * ng, cudaMemcpyHostToDevice));
+        cap = cap_planes;
+        mid.alloc((size_t)cap * ng * ng);
+        tc = pick_tile<T>(ng);
+        sc = (T)(1.0 / std::sqrt((double)ng));
+    }
+
+    template <class LD, class ST>
+    void spctop(cudaStream_t s, int nout, LD ld, ST st) const {
+        for (int o0 = 0; o0 < nout; o0 += cap) {
+            const int cnt = (nout - o0 < cap) ? nout - o0 : cap;
+            launch_pass<T, true, true, false>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidPC<T>{mid.p, ng});
+            launch_pass<T, true, true, true>(s, plan, tw.p, tc, sc, cnt, ng, MidCP<T>{mid.p, ng}, StOff<ST>{st, o0});
+        }
+    }
+    template <class LD, class ST>
+    void ptospc(cudaStream_t s, int nout, LD ld, ST st) const {
+        for (int o0 = 0; o0 < nout; o0 += cap) {
+            const int cnt = (nout - o0 < cap) ? nout - o0 : cap;
+            launch_pass<T, false, true, true>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidCP<T>{mid.p, ng});
+            launch_pass<T, false, false, true>(s, plan, tw.p, tc, sc, cnt, ng, MidPC<T>{mid.p, ng}, StOff<ST>{st, o0});
+        }
+    }
+};
+
+// Spectral derivative helpers (D2FFT::xderiv/yderiv, src/sta2dfft.rs:128-184):
+// d/dx at Hermitian index a is dmul(a) * var[mirror(a)] along that axis.
+__device__ __forceinline__ int mirror(int a, int ng) { return a == 0 ? 0 : ng - a; }
+__device__ __forceinline__ double dmul(int a, int ng) {
+    return (a == 0 || 2 * a == ng) ? 0.0 : ((2 * a < ng) ? -(double)a : (double)(ng - a));
+}
+// Parseval weight of one axis for the Hermitian packing: 1 at 0 and ng/2, else 2.
+__device__ __forceinline__ double pweight(int a, int ng) { return (a == 0 || 2 * a == ng) ? 1.0 : 2.0; }
+
+}  // namespace sw

@@ -1,0 +1,977 @@
+// The nhswps time-step path on the GPU: main_invert, vertical, coeffs,
+// cpsource, psolve, source, advance, diagnose and the savegrid energies for an
+// ensemble of M independent members of one (ng, nz) grid.
+//
+// Every 3-D field is stored member-major in the reference's Fortran order:
+// plane q = m*(nz+1) + iz holds ng*ng values, physical p[iy + ng*ix] or spectral
+// s[kx + ng*ky].  T is the precision of the transforms and of the physical
+// work fields (double for SW_FP64, float for SW_MIXED); the prognostic spectral
+// fields qs, ds, gs, the pressure ps, the tridiagonal solves, the residual, the
+// diagnostics and the time update are float64 in both paths.
+#pragma once
+#include <algorithm>
+#include <map>
+#include <memory>
+
+#include "sw_fft2d.cuh"
+#include "sw_spectral_host.h"
+
+namespace sw {
+
+struct DeviceOps {
+    DevBuf<double> hlap, glap, rlap, helm, c2g2, simp, rope, fope, filt, diss, opak, rdis, ap;
+    DevBuf<double> htdv, etdv, weight, theta, htd1, etd1;
+};
+
+inline void upload(DevBuf<double>& d, const std::vector<double>& h) {
+    d.alloc(h.size());
+    SW_CUDA(cudaMemcpy(d.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+}
+
+template <typename T>
+struct Solver {
+    int ng, nz, L, M, n2, ML;
+    size_t nf;  // elements of one 3-D field for all members
+    double t = 0.0;
+    cudaStream_t st = nullptr;
+    SpectralHost host;
+    DeviceOps op;
+    Fft2d<T> fft;
+
+    // state (src/nhswps/mod.rs:87-148)
+    DevBuf<T> u, v, w, z, zx, zy, r, ri, aa, zeta, pn, dpn;
+    DevBuf<double> ps, qs, ds, gs;
+    // persistent psolve coefficients
+    DevBuf<T> sigx, sigy, cpt1, cpt2, sp0;
+    // work fields
+    std::vector<DevBuf<T>> wt;       // T-precision 3-D work fields
+    std::vector<DevBuf<double>> wd;  // float64 3-D work fields (advance, psolve)
+    DevBuf<double> plane_d;          // M*n2 float64 per-member planes (x4)
+    DevBuf<T> plane_t;               // M*n2 T per-member planes (x4)
+    DevBuf<double> red_partial, red_out;
+    DevBuf<double> errp_d, diag_hist;
+    DevBuf<int> ctrl;  // per member: active, iters, status
+    double* h_pinned = nullptr;  // host staging for small readbacks
+    int hist_cap = 4096, hist_rows = 0;
+    int last_sweeps[3] = {0, 0, 0};
+
+    static constexpr int NWT = 24;
+    static constexpr int NWD = 12;
+
+    Solver(int ng_, int nz_, int M_) : ng(ng_), nz(nz_), L(nz_ + 1), M(M_), n2(ng_ * ng_), ML(M_ * (nz_ + 1)) {
+        require(ng >= 4 && ng % 2 == 0, SW_ERR_ARG, "ng must be even and >= 4");
+        require(nz >= 2 && nz <= MAX_NZ, SW_ERR_ARG, "nz must be in [2, 128]");
+        require(M >= 1, SW_ERR_ARG, "nmembers must be >= 1");
+        FftPlan tmp;
+        require(build_plan(ng, tmp) == SW_OK, SW_ERR_FACTORISE, "ng must factor into 2, 3 and 5");
+        nf = (size_t)M * L * n2;
+        SW_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        host.build(ng, nz);
+        upload(op.hlap, host.hlap); upload(op.glap, host.glap); upload(op.rlap, host.rlap);
+        upload(op.helm, host.helm); upload(op.c2g2, host.c2g2); upload(op.simp, host.simp);
+        upload(op.rope, host.rope); upload(op.fope, host.fope); upload(op.filt, host.filt);
+        upload(op.diss, host.diss); upload(op.opak, host.opak); upload(op.rdis, host.rdis);
+        upload(op.ap, host.ap); upload(op.htdv, host.htdv); upload(op.etdv, host.etdv);
+        upload(op.weight, host.weight); upload(op.theta, host.theta);
+        upload(op.htd1, host.htd1); upload(op.etd1, host.etd1);
+        fft.init(ng, 6 * ML);
+        for (auto* b : {&u, &v, &w, &z, &zx, &zy, &r, &ri, &aa, &zeta, &pn, &dpn, &sigx, &sigy, &cpt1, &cpt2, &sp0}) {
+            b->alloc(nf);
+            SW_CUDA(cudaMemset(b->p, 0, nf * sizeof(T)));
+        }
+        for (auto* b : {&ps, &qs, &ds, &gs}) {
+            b->alloc(nf);
+            SW_CUDA(cudaMemset(b->p, 0, nf * sizeof(double)));
+        }
+        wt.resize(NWT);
+        for (auto& b : wt) b.alloc(nf);
+        wd.resize(NWD);
+        for (auto& b : wd) b.alloc(nf);
+        plane_d.alloc((size_t)4 * M * n2);
+        plane_t.alloc((size_t)4 * M * n2);
+        red_partial.alloc((size_t)RED_CHUNKS * 8 * ML + 64);
+        red_out.alloc((size_t)8 * ML + 64);
+        errp_d.alloc((size_t)2 * M + 2);
+        diag_hist.alloc((size_t)hist_cap * M * 3);
+        ctrl.alloc((size_t)3 * M + 1);
+        SW_CUDA(cudaMallocHost(&h_pinned, sizeof(double) * (16 * (size_t)M + 64)));
+    }
+    ~Solver() {
+        if (st) cudaStreamSynchronize(st);
+        if (h_pinned) cudaFreeHost(h_pinned);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    T* W(int i) { return wt[i].p; }
+    double* WD(int i) { return wd[i].p; }
+    T* field_t(int f) {
+        switch (f) {
+            case SW_U: return u; case SW_V: return v; case SW_W: return w; case SW_Z: return z;
+            case SW_ZX: return zx; case SW_ZY: return zy; case SW_R: return r; case SW_RI: return ri;
+            case SW_AA: return aa; case SW_ZETA: return zeta; case SW_PN: return pn; case SW_DPN: return dpn;
+            default: return nullptr;
+        }
+    }
+    double* field_d(int f) {
+        switch (f) {
+            case SW_PS: return ps; case SW_QS: return qs; case SW_DS: return ds; case SW_GS: return gs;
+            default: return nullptr;
+        }
+    }
+
+    // ======================================================================
+    // main_invert (src/spectral/mod.rs:305-417)
+    // ======================================================================
+    void main_invert() {
+        const int ng = this->ng, n2 = this->n2, L = this->L, ML = this->ML;
+        const double *QS = qs, *DS = ds, *GS = gs, *rope = op.rope, *rlap = op.rlap, *wgt = op.weight;
+        double* wkh = plane_d.p;
+        // vertical average of eta = gamma/f^2 - q/f, times rope
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            double s = 0.0;
+            for (int iz = 0; iz < L; iz++) {
+                const size_t p = (size_t)(m * L + iz) * n2 + i;
+                s += wgt[iz] * (COFI * (COFI * GS[p] - QS[p]));
+            }
+            wkh[c] = s * rope[i];
+        });
+        T *R = r, *U = u, *V = v, *ZE = zeta;
+        fft.spctop(st, 4 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / ML, q = o - which * ML, m = q / L;
+                const double* qsq = QS + (size_t)q * n2;
+                const double* dsq = DS + (size_t)q * n2;
+                const double* gsq = GS + (size_t)q * n2;
+                const double* wk = wkh + (size_t)m * n2;
+                auto wka = [&](int i) { return COFI * (COFI * gsq[i] - qsq[i]) - wk[i]; };
+                auto wkb = [&](int i) { return qsq[i] + COF * wka(i); };
+                const int i = kx + ng * ky;
+                if (which == 0) return (T)wka(i);
+                if (which == 1) return (T)wkb(i);
+                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+                if (which == 2)
+                    return (T)(dmul(kx, ng) * (rlap[mx] * dsq[mx]) - dmul(ky, ng) * (rlap[my] * wkb(my)));
+                return (T)(dmul(ky, ng) * (rlap[my] * dsq[my]) + dmul(kx, ng) * (rlap[mx] * wkb(mx)));
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / ML, q = o - which * ML;
+                T* out = which == 0 ? R : which == 1 ? ZE : which == 2 ? U : V;
+                out[(size_t)q * n2 + iy + ng * ix] = val;
+            });
+        // mean flow (uio, vio): per-plane sums of u*r and v*r
+        double* sums = red_out.p;
+        reduce_groups<2>(st, ML, n2, 0u,
+            [=] __device__(int g, long long i) {
+                const size_t p = (size_t)g * n2 + i;
+                RedVals<2> rv;
+                rv.v[0] = (double)U[p] * (double)R[p];
+                rv.v[1] = (double)V[p] * (double)R[p];
+                return rv;
+            }, red_partial.p, sums);
+        const double dsumi = 1.0 / (double)(ng * ng);
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L;
+            double uio = 0.0, vio = 0.0;
+            for (int iz = 0; iz < L; iz++) {
+                uio -= wgt[iz] * sums[2 * (m * L + iz)] * dsumi;
+                vio -= wgt[iz] * sums[2 * (m * L + iz) + 1] * dsumi;
+            }
+            const size_t p = (size_t)q * n2 + i;
+            U[p] = (T)((double)U[p] + uio);
+            V[p] = (T)((double)V[p] + vio);
+        });
+    }
+
+    // ======================================================================
+    // vertical (src/nhswps/vertical.rs:8-143)
+    // ======================================================================
+    void vertical() {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+        const double dz2 = (HBAR / (double)nz) / 2.0;
+        const double *theta = op.theta, *filt = op.filt, *DS = ds;
+        T *Z = z, *R = r, *U = u, *V = v, *WW = w, *ZX = zx, *ZY = zy, *AA = aa;
+        T *S1 = W(0), *SA = W(1), *SB = W(2), *RS = W(3);
+        // z by trapezoidal integration of rho'_theta, then + theta
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            T* zc = Z + (size_t)m * L * n2 + i;
+            const T* rc = R + (size_t)m * L * n2 + i;
+            double prev = dz2 * ((double)rc[0] + (double)rc[n2]);
+            zc[n2] = (T)prev;
+            for (int iz = 1; iz < nz; iz++) {
+                prev = prev + dz2 * ((double)rc[(size_t)iz * n2] + (double)rc[(size_t)(iz + 1) * n2]);
+                zc[(size_t)(iz + 1) * n2] = (T)prev;
+            }
+            for (int iz = 1; iz <= nz; iz++) zc[(size_t)iz * n2] = (T)((double)zc[(size_t)iz * n2] + theta[iz]);
+        });
+        // z_x, z_y for iz = 1..nz
+        const int Mnz = M * nz;
+        fft.ptospc(st, Mnz,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int m = o / nz, iz = 1 + o % nz;
+                return Z[(size_t)(m * L + iz) * n2 + iy + ng * ix];
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int m = o / nz, iz = 1 + o % nz;
+                S1[(size_t)(m * L + iz) * n2 + kx + ng * ky] = val;
+            });
+        fft.spctop(st, 2 * Mnz,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / Mnz, q = o - which * Mnz, m = q / nz, iz = 1 + q % nz;
+                const T* s = S1 + (size_t)(m * L + iz) * n2;
+                if (which == 0) return (T)(dmul(kx, ng) * (double)s[mirror(kx, ng) + ng * ky]);
+                return (T)(dmul(ky, ng) * (double)s[kx + ng * mirror(ky, ng)]);
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / Mnz, q = o - which * Mnz, m = q / nz, iz = 1 + q % nz;
+                (which == 0 ? ZX : ZY)[(size_t)(m * L + iz) * n2 + iy + ng * ix] = val;
+            });
+        // A = filt * (d/dx(u r) + d/dy(v r))
+        fft.ptospc(st, 2 * ML,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int which = o / ML, q = o - which * ML;
+                const size_t p = (size_t)q * n2 + iy + ng * ix;
+                return (which == 0 ? U[p] : V[p]) * R[p];
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int which = o / ML, q = o - which * ML;
+                (which == 0 ? SA : SB)[(size_t)q * n2 + kx + ng * ky] = val;
+            });
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int kx = i % ng, ky = i / ng;
+            const T* a = SA + (size_t)q * n2;
+            const T* b = SB + (size_t)q * n2;
+            const double wkb = dmul(kx, ng) * (double)a[mirror(kx, ng) + ng * ky];
+            const double wkc = dmul(ky, ng) * (double)b[kx + ng * mirror(ky, ng)];
+            AA[(size_t)q * n2 + i] = (T)(filt[i] * (wkb + wkc));
+        });
+        // rsrc = -(A + delta) in physical space
+        fft.spctop(st, ML,
+            [=] __device__(int q, int kx, int ky) -> T {
+                const size_t p = (size_t)q * n2 + kx + ng * ky;
+                return (T)((double)AA[p] + DS[p]);
+            },
+            [=] __device__(int q, int iy, int ix, T val) { RS[(size_t)q * n2 + iy + ng * ix] = -val; });
+        // w by trapezoidal integration
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            T* wc = WW + (size_t)m * L * n2 + i;
+            const T* sc = RS + (size_t)m * L * n2 + i;
+            double prev = dz2 * ((double)sc[0] + (double)sc[n2]);
+            wc[n2] = (T)prev;
+            for (int iz = 1; iz < nz; iz++) {
+                prev = prev + dz2 * ((double)sc[(size_t)iz * n2] + (double)sc[(size_t)(iz + 1) * n2]);
+                wc[(size_t)(iz + 1) * n2] = (T)prev;
+            }
+        });
+        // w += deal(u z_x + v z_y), iz = 1..nz
+        fft.ptospc(st, Mnz,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int m = o / nz, iz = 1 + o % nz;
+                const size_t p = (size_t)(m * L + iz) * n2 + iy + ng * ix;
+                return U[p] * ZX[p] + V[p] * ZY[p];
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int m = o / nz, iz = 1 + o % nz;
+                const int i = kx + ng * ky;
+                S1[(size_t)(m * L + iz) * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        fft.spctop(st, Mnz,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int m = o / nz, iz = 1 + o % nz;
+                return S1[(size_t)(m * L + iz) * n2 + kx + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int m = o / nz, iz = 1 + o % nz;
+                const size_t p = (size_t)(m * L + iz) * n2 + iy + ng * ix;
+                WW[p] = WW[p] + val;
+            });
+    }
+
+    // ======================================================================
+    // coeffs (src/nhswps/coeffs.rs:8-101): sigx, sigy (x2), cpt1, cpt2
+    // ======================================================================
+    void coeffs() {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, ML = this->ML;
+        const double qdzi = (1.0 / 4.0) * (1.0 / (HBAR / (double)nz));
+        const double* filt = op.filt;
+        T *RI = ri, *ZX = zx, *ZY = zy, *SX = sigx, *SY = sigy, *C1 = cpt1, *C2 = cpt2;
+        T *Sx = W(4), *Sy = W(5), *Sc = W(6), *D = W(7);
+        fft.ptospc(st, 2 * ML,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int which = o / ML, q = o - which * ML;
+                const size_t p = (size_t)q * n2 + iy + ng * ix;
+                return RI[p] * (which == 0 ? ZX[p] : ZY[p]);
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int which = o / ML, q = o - which * ML, i = kx + ng * ky;
+                (which == 0 ? Sx : Sy)[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        fft.spctop(st, 2 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / ML, q = o - which * ML;
+                return (which == 0 ? Sx : Sy)[(size_t)q * n2 + kx + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / ML, q = o - which * ML;
+                (which == 0 ? SX : SY)[(size_t)q * n2 + iy + ng * ix] = val;
+            });
+        fft.ptospc(st, ML,
+            [=] __device__(int q, int iy, int ix) -> T {
+                const size_t p = (size_t)q * n2 + iy + ng * ix;
+                return T(1) - RI[p] * RI[p] - SX[p] * SX[p] - SY[p] * SY[p];
+            },
+            [=] __device__(int q, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                Sc[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        // cpt2 = deal(...) (all levels), D = div(sig) for iz >= 1
+        fft.spctop(st, 2 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / ML, q = o - which * ML;
+                if (which == 0) return Sc[(size_t)q * n2 + kx + ng * ky];
+                const T* a = Sx + (size_t)q * n2;
+                const T* b = Sy + (size_t)q * n2;
+                return (T)(dmul(ky, ng) * (double)b[kx + ng * mirror(ky, ng)] +
+                           dmul(kx, ng) * (double)a[mirror(kx, ng) + ng * ky]);
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / ML, q = o - which * ML;
+                (which == 0 ? C2 : D)[(size_t)q * n2 + iy + ng * ix] = val;
+            });
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L, iz = q % L;
+            const T* c2 = C2 + (size_t)m * L * n2 + i;
+            const size_t p = (size_t)q * n2 + i;
+            double val;
+            if (iz == 0)
+                val = qdzi * (4.0 * (double)c2[n2] - 3.0 * (double)c2[0] - (double)c2[2 * (size_t)n2]);
+            else if (iz < nz)
+                val = qdzi * ((double)c2[(size_t)(iz + 1) * n2] - (double)c2[(size_t)(iz - 1) * n2]) + (double)D[p];
+            else
+                val = qdzi * (3.0 * (double)c2[(size_t)nz * n2] + (double)c2[(size_t)(nz - 2) * n2] -
+                              4.0 * (double)c2[(size_t)(nz - 1) * n2]) + (double)D[p];
+            C1[p] = (T)val;
+            SX[p] = SX[p] * T(2);
+            SY[p] = SY[p] * T(2);
+        });
+    }
+
+    // theta-derivative of a level field at level iz (cpsource.rs:46-103)
+    static __device__ __forceinline__ double tderiv(const T* col, int iz, int nz, int n2, double hdzi) {
+        if (iz == 0) return hdzi * (4.0 * (double)col[n2] - 3.0 * (double)col[0] - (double)col[2 * (size_t)n2]);
+        if (iz == nz)
+            return hdzi * (3.0 * (double)col[(size_t)nz * n2] + (double)col[(size_t)(nz - 2) * n2] -
+                           4.0 * (double)col[(size_t)(nz - 1) * n2]);
+        return hdzi * ((double)col[(size_t)(iz + 1) * n2] - (double)col[(size_t)(iz - 1) * n2]);
+    }
+
+    // ======================================================================
+    // cpsource (src/nhswps/cpsource.rs:13-261): sp0
+    // Work: W(8..10) spectral u,v,w; W(11..16) ux,uy,vx,vy,wx,wy; W(17..19)
+    // spectral/physical wkp,wkq,wkr; plane_t = hsrc.
+    // ======================================================================
+    void cpsource() {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+        const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
+        const double *filt = op.filt, *glap = op.glap;
+        T *Z = z, *U = u, *V = v, *WW = w, *RI = ri, *ZE = zeta, *ZX = zx, *ZY = zy, *SP0 = sp0;
+        T *Su = W(8), *Sv = W(9), *Sw = W(10);
+        T *UX = W(11), *UY = W(12), *VX = W(13), *VY = W(14), *WX = W(15), *WY = W(16);
+        T *Pp = W(17), *Pq = W(18), *Pr = W(19);
+        T* hs = plane_t.p;        // M planes: spectral then physical hsrc
+        T* hsrc = plane_t.p + (size_t)M * n2;
+        // hsrc = -g Lap(h) in physical space
+        fft.ptospc(st, M,
+            [=] __device__(int m, int iy, int ix) -> T { return Z[(size_t)(m * L + nz) * n2 + iy + ng * ix]; },
+            [=] __device__(int m, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                hs[(size_t)m * n2 + i] = (T)((double)val * glap[i]);
+            });
+        fft.spctop(st, M,
+            [=] __device__(int m, int kx, int ky) -> T { return hs[(size_t)m * n2 + kx + ng * ky]; },
+            [=] __device__(int m, int iy, int ix, T val) { hsrc[(size_t)m * n2 + iy + ng * ix] = val; });
+        // horizontal derivatives of u, v, w
+        fft.ptospc(st, 3 * ML,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int which = o / ML, q = o - which * ML;
+                const size_t p = (size_t)q * n2 + iy + ng * ix;
+                return which == 0 ? U[p] : which == 1 ? V[p] : WW[p];
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int which = o / ML, q = o - which * ML;
+                (which == 0 ? Su : which == 1 ? Sv : Sw)[(size_t)q * n2 + kx + ng * ky] = val;
+            });
+        fft.spctop(st, 6 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / ML, q = o - which * ML;
+                const T* s = (which < 2 ? Su : which < 4 ? Sv : Sw) + (size_t)q * n2;
+                if ((which & 1) == 0) return (T)(dmul(kx, ng) * (double)s[mirror(kx, ng) + ng * ky]);
+                return (T)(dmul(ky, ng) * (double)s[kx + ng * mirror(ky, ng)]);
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / ML, q = o - which * ML;
+                T* out = which == 0 ? UX : which == 1 ? UY : which == 2 ? VX : which == 3 ? VY : which == 4 ? WX : WY;
+                out[(size_t)q * n2 + iy + ng * ix] = val;
+            });
+        // dealiased products wkp (iz>=1), wkq (all iz), wkr (iz>=1)
+        fft.ptospc(st, 3 * ML,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int which = o / ML, q = o - which * ML, m = q / L, iz = q % L;
+                const int i = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + i;
+                const size_t cb = (size_t)m * L * n2 + i;
+                const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
+                if (which == 1 && iz == 0) return (T)((double)RI[p] * wt);
+                if (iz == 0) return T(0);
+                const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
+                const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
+                if (which == 0) return (T)(vt * (double)ZX[p] - ut * (double)ZY[p]);
+                if (which == 1) return (T)((double)UY[p] * vt - ut * (double)VY[p]);
+                return (T)(ut * (double)VX[p] - (double)UX[p] * vt);
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int which = o / ML, q = o - which * ML, i = kx + ng * ky;
+                (which == 0 ? Su : which == 1 ? Sv : Sw)[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        fft.spctop(st, 3 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / ML, q = o - which * ML;
+                return (which == 0 ? Su : which == 1 ? Sv : Sw)[(size_t)q * n2 + kx + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / ML, q = o - which * ML;
+                (which == 0 ? Pp : which == 1 ? Pq : Pr)[(size_t)q * n2 + iy + ng * ix] = val;
+            });
+        // second dealiased product (iz >= 1), then sp0
+        fft.ptospc(st, ML,
+            [=] __device__(int q, int iy, int ix) -> T {
+                const int m = q / L, iz = q % L;
+                if (iz == 0) return T(0);
+                const int i = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + i;
+                const size_t cb = (size_t)m * L * n2 + i;
+                const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
+                const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
+                const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
+                double wkq = (double)Pq[p] * (double)ZX[p] + (double)Pr[p] * (double)ZY[p] - (double)WY[p] * vt;
+                wkq += ((double)UX[p] + (double)VY[p]) * wt - (double)WX[p] * ut;
+                return (T)wkq;
+            },
+            [=] __device__(int q, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                Sw[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        fft.spctop(st, ML,
+            [=] __device__(int q, int kx, int ky) -> T { return Sw[(size_t)q * n2 + kx + ng * ky]; },
+            [=] __device__(int q, int iy, int ix, T val) {
+                const int m = q / L, iz = q % L;
+                const int i = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + i;
+                const double hsv = (double)hsrc[(size_t)m * n2 + i];
+                const double ux = UX[p], uy = UY[p], vx = VX[p], vy = VY[p];
+                double s;
+                if (iz == 0) {
+                    const double wkq = Pq[p];
+                    s = hsv + COF * (double)ZE[p];
+                    s += 2.0 * (ux * vy - uy * vx + wkq * (ux + vy));
+                } else {
+                    const double rip = RI[p];
+                    s = hsv + COF * ((double)ZE[p] - rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
+                    s += 2.0 * (ux * vy - uy * vx);
+                }
+                SP0[p] = (T)s;
+            });
+    }
+
+    // ======================================================================
+    // psolve (src/nhswps/psolve.rs:16-411)
+    // Work: W(0..3) A,B,C,D physical sweep terms; W(4) sp (spectral source);
+    // WD(0) psa (previous spectral pressure), WD(1) compact RHS for dp/dtheta.
+    // ctrl: [active, iters, status] per member; errp_d: errp per member.
+    // Returns member-0 status.
+    // ======================================================================
+    int psolve(int nitmax, int* iters_out, double* errp_out) {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+        require(nz >= 3, SW_ERR_ARG, "psolve needs nz >= 3");
+        if (nitmax <= 0) nitmax = 100;
+        const double toler = 1.0E-9;
+        const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz2 = dz / 2.0, dz6 = dz / 6.0;
+        const double dzisq = (1.0 / dz) * (1.0 / dz);
+        const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
+        const double *filt = op.filt, *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap, *htd1 = op.htd1, *etd1 = op.etd1;
+        T *R = r, *RI = ri, *PN = pn, *DPN = dpn;
+        double* PS = ps;
+        // ri = 1/(1+r), dealiased
+        T* Sr = W(0);
+        fft.ptospc(st, ML,
+            [=] __device__(int q, int iy, int ix) -> T { return T(1) / (R[(size_t)q * n2 + iy + ng * ix] + T(1)); },
+            [=] __device__(int q, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                Sr[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        fft.spctop(st, ML,
+            [=] __device__(int q, int kx, int ky) -> T { return Sr[(size_t)q * n2 + kx + ng * ky]; },
+            [=] __device__(int q, int iy, int ix, T val) { RI[(size_t)q * n2 + iy + ng * ix] = val; });
+        vertical();
+        coeffs();
+        cpsource();
+        T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
+        T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
+        double* PSA = WD(0);
+        int* ctl = ctrl.p;
+        double* errp = errp_d.p;
+        // spectral pressure of the first guess: psa = ptospc(pn) (all levels), ps = psa with ps(nz) = 0
+        fft.ptospc(st, ML,
+            [=] __device__(int q, int iy, int ix) -> T { return PN[(size_t)q * n2 + iy + ng * ix]; },
+            [=] __device__(int q, int kx, int ky, T val) {
+                const int iz = q % L;
+                const size_t p = (size_t)q * n2 + kx + ng * ky;
+                PSA[p] = (double)val;
+                PS[p] = (iz == nz) ? 0.0 : (double)val;
+            });
+        for_cols(st, M, [=] __device__(int m) {
+            ctl[3 * m] = 1;
+            ctl[3 * m + 1] = 0;
+            ctl[3 * m + 2] = SW_OK;
+        });
+        const int nsp = 4 * nz - 1;  // spctop outputs per member per sweep
+        int sweeps = 0;
+        while (true) {
+            // (a) pressure derivative terms to physical space
+            fft.spctop(st, M * nsp,
+                [=] __device__(int o, int kx, int ky) -> T {
+                    const int m = o / nsp, k = o - m * nsp;
+                    const double* pc = PS + (size_t)m * L * n2 + kx + ng * ky;
+                    auto P = [&](int iz, int dx, int dy) {
+                        const int jx = dx ? mirror(kx, ng) : kx, jy = dy ? mirror(ky, ng) : ky;
+                        return pc[(size_t)iz * n2 + (jx - kx) + ng * (jy - ky)];
+                    };
+                    auto wka = [&](int iz, int dx, int dy) { return (P(iz + 1, dx, dy) - P(iz - 1, dx, dy)) * hdzi; };
+                    auto wkd = [&](int iz, int dx, int dy) {
+                        return (P(iz + 1, dx, dy) - 2.0 * P(iz, dx, dy) + P(iz - 1, dx, dy)) * dzisq;
+                    };
+                    if (k == 0) return (T)((2.0 * P(0, 0, 0) - 5.0 * P(1, 0, 0) + 4.0 * P(2, 0, 0) - P(3, 0, 0)) * dzisq);
+                    if (k < 4 * nz - 3) {
+                        const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
+                        if (kind == 0) return (T)(dmul(kx, ng) * wka(iz, 1, 0));
+                        if (kind == 1) return (T)(dmul(ky, ng) * wka(iz, 0, 1));
+                        if (kind == 2) return (T)wka(iz, 0, 0);
+                        return (T)wkd(iz, 0, 0);
+                    }
+                    // extrapolated dp/dtheta at iz = nz (spectral form of psolve.rs:232-238)
+                    const int dx = (k == 4 * nz - 3), dy = !dx;
+                    const double sa = wka(nz - 1, dx, dy) + dz2 * (3.0 * wkd(nz - 1, dx, dy) - wkd(nz - 2, dx, dy));
+                    return (T)((dx ? dmul(kx, ng) : dmul(ky, ng)) * sa);
+                },
+                [=] __device__(int o, int iy, int ix, T val) {
+                    const int m = o / nsp, k = o - m * nsp;
+                    const size_t base = (size_t)m * L * n2 + iy + ng * ix;
+                    if (k == 0) { D[base] = val; return; }
+                    if (k < 4 * nz - 3) {
+                        const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
+                        T* out = kind == 0 ? A : kind == 1 ? B : kind == 2 ? C : D;
+                        out[base + (size_t)iz * n2] = val;
+                        return;
+                    }
+                    ((k == 4 * nz - 3) ? A : B)[base + (size_t)nz * n2] = val;
+                });
+            // (b) total source S = S0 + S1(p), to spectral space
+            fft.ptospc(st, ML,
+                [=] __device__(int q, int iy, int ix) -> T {
+                    const int m = q / L, iz = q % L;
+                    const int i = iy + ng * ix;
+                    const size_t p = (size_t)q * n2 + i;
+                    const size_t cb = (size_t)m * L * n2 + i;
+                    double s;
+                    if (iz == 0) {
+                        s = (double)SP0[p] + (double)C2[p] * (double)D[p];
+                    } else if (iz < nz) {
+                        s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
+                        s += (double)C2[p] * (double)D[p] + (double)C1[p] * (double)C[p];
+                    } else {
+                        const double d1 = D[cb + (size_t)(nz - 1) * n2], d2 = D[cb + (size_t)(nz - 2) * n2];
+                        const double dpdt = (double)C[cb + (size_t)(nz - 1) * n2] + dz2 * (3.0 * d1 - d2);
+                        const double d2pdt2 = 2.0 * d1 - d2;
+                        s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
+                        s += (double)C2[p] * d2pdt2 + (double)C1[p] * dpdt;
+                    }
+                    return (T)s;
+                },
+                [=] __device__(int q, int kx, int ky, T val) { SP[(size_t)q * n2 + kx + ng * ky] = val; });
+            // (c) compact RHS and Thomas solve per (kx, ky) column; residual terms
+            double* cterm = WD(1);  // per column: [num, den] packed as two planes of M*n2
+            for_cols(st, M * n2, [=] __device__(int c) {
+                const int m = c / n2, i = c - m * n2;
+                const size_t cb = (size_t)m * L * n2 + i;
+                double* num = cterm + c;
+                double* den = cterm + (size_t)M * n2 + c;
+                if (!ctl[3 * m]) { *num = 0.0; *den = 0.0; return; }
+                double sp[MAX_NZ + 1], x[MAX_NZ + 1];
+                for (int iz = 0; iz <= nz; iz++) sp[iz] = (double)SP[cb + (size_t)iz * n2];
+                const double api = ap[i];
+                x[0] = ((1.0 / 3.0) * sp[0] + (1.0 / 6.0) * sp[1]) * htdv[i];
+                for (int iz = 1; iz < nz; iz++) {
+                    const double g = (1.0 / 12.0) * (sp[iz - 1] + sp[iz + 1]) + (5.0 / 6.0) * sp[iz];
+                    x[iz] = (g - api * x[iz - 1]) * htdv[i + (size_t)n2 * iz];
+                }
+                for (int iz = nz - 2; iz >= 0; iz--) x[iz] += etdv[i + (size_t)n2 * iz] * x[iz + 1];
+                x[nz] = 0.0;
+                const int kx = i % ng, ky = i / ng;
+                const double wgt = pweight(kx, ng) * pweight(ky, ng);
+                double sn = 0.0, sd = 0.0;
+                for (int iz = 0; iz <= nz; iz++) {
+                    const size_t p = cb + (size_t)iz * n2;
+                    const double old = PSA[p];
+                    sn += (x[iz] - old) * (x[iz] - old);
+                    sd += old * old;
+                    PS[p] = x[iz];
+                    PSA[p] = x[iz];
+                }
+                *num = wgt * sn;
+                *den = wgt * sd;
+            });
+            reduce_groups<2>(st, M, n2, 0u,
+                [=] __device__(int g, long long i) {
+                    RedVals<2> rv;
+                    rv.v[0] = cterm[(size_t)g * n2 + i];
+                    rv.v[1] = cterm[(size_t)M * n2 + (size_t)g * n2 + i];
+                    return rv;
+                }, red_partial.p, red_out.p);
+            // (d) convergence control (psolve.rs:89, 339-358)
+            const double* sums = red_out.p;
+            for_cols(st, M, [=] __device__(int m) {
+                if (!ctl[3 * m]) return;
+                const double e = sqrt(sums[2 * m] / (sums[2 * m + 1] + 1.0E-20));
+                errp[m] = e;
+                const int it = ctl[3 * m + 1];
+                if (it > 0 && e > 1.0) {
+                    ctl[3 * m + 2] = SW_ERR_PSOLVE_DIVERGED;
+                    ctl[3 * m] = 0;
+                    ctl[3 * m + 1] = it + 1;
+                    return;
+                }
+                ctl[3 * m + 1] = it + 1;
+                if (!(e > toler) || it + 1 >= nitmax) {
+                    ctl[3 * m] = 0;
+                    if (it + 1 >= nitmax) ctl[3 * m + 2] = SW_ERR_PSOLVE_MAXITER;
+                }
+            });
+            sweeps++;
+            int* hctl = reinterpret_cast<int*>(h_pinned);
+            SW_CUDA(cudaMemcpyAsync(hctl, ctl, sizeof(int) * 3 * M, cudaMemcpyDeviceToHost, st));
+            SW_CUDA(cudaStreamSynchronize(st));
+            bool any = false;
+            for (int m = 0; m < M; m++) any = any || hctl[3 * m];
+            if (!any || sweeps >= nitmax) break;
+        }
+        int* hctl = reinterpret_cast<int*>(h_pinned);
+        const int status0 = hctl[2];
+        int worst = SW_OK;
+        for (int m = 0; m < M; m++)
+            if (hctl[3 * m + 2] != SW_OK) worst = hctl[3 * m + 2];
+        if (iters_out) *iters_out = hctl[1];
+        if (errp_out) SW_CUDA(cudaMemcpy(errp_out, errp, sizeof(double), cudaMemcpyDeviceToHost));
+        last_psolve_iters = hctl[1];
+        if (worst != SW_OK) return worst;
+        // pn = spctop(ps), levels 0..nz-1; pn(nz) = 0
+        fft.spctop(st, ML,
+            [=] __device__(int q, int kx, int ky) -> T { return (T)PS[(size_t)q * n2 + kx + ng * ky]; },
+            [=] __device__(int q, int iy, int ix, T val) {
+                PN[(size_t)q * n2 + iy + ng * ix] = (q % L == nz) ? T(0) : val;
+            });
+        // dp/dtheta by 4th-order compact differences (psolve.rs:371-410), levels 1..nz
+        double* GG = WD(1);
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            const size_t cb = (size_t)m * L * n2 + i;
+            double g[MAX_NZ + 1];
+            auto P = [&](int iz) { return PS[cb + (size_t)iz * n2]; };
+            for (int iz = 1; iz < nz; iz++) g[iz] = (P(iz + 1) - P(iz - 1)) * hdzi;
+            g[nz] = dz6 * (double)SP[cb + (size_t)nz * n2] - P(nz - 1) * dzi;
+            g[1] *= htd1[0];
+            for (int iz = 2; iz < nz; iz++) g[iz] = (g[iz] - (1.0 / 6.0) * g[iz - 1]) * htd1[iz - 1];
+            g[nz] = (g[nz] - (1.0 / 3.0) * g[nz - 1]) * htd1[nz - 1];
+            for (int iz = nz - 1; iz >= 1; iz--) g[iz] += etd1[iz - 1] * g[iz + 1];
+            for (int iz = 1; iz <= nz; iz++) GG[cb + (size_t)iz * n2] = g[iz];
+        });
+        const int Mnz = M * nz;
+        fft.spctop(st, Mnz,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int m = o / nz, iz = 1 + o % nz;
+                return (T)GG[(size_t)(m * L + iz) * n2 + kx + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int m = o / nz, iz = 1 + o % nz;
+                DPN[(size_t)(m * L + iz) * n2 + iy + ng * ix] = val;
+            });
+        return status0;
+    }
+    int last_psolve_iters = 0;
+
+    // ======================================================================
+    // source (src/nhswps/source.rs:19-138) -> sqs, sds, sgs (float64)
+    // Work: W(5..6) q, dd; W(7) F spectral; W(8..10) ff, ffx, ffy; W(11..14)
+    // ux, uy, vx, vy; W(15..16) spectral u, v; W(17..22) product spectra;
+    // plane_t: z derivatives at iz = 0.
+    // ======================================================================
+    void source(double* SQS, double* SDS, double* SGS) {
+        const int ng = this->ng, n2 = this->n2, L = this->L, M = this->M, ML = this->ML;
+        const double *filt = op.filt, *hlap = op.hlap, *c2g2 = op.c2g2, *wgt = op.weight;
+        const double *QS = qs, *DS = ds, *PSp = ps;
+        T *U = u, *V = v, *RI = ri, *DPN = dpn, *Z = z, *ZX = zx, *ZY = zy, *AA = aa;
+        T *Q = W(5), *DD = W(6), *F = W(7), *FF = W(8), *FX = W(9), *FY = W(10);
+        T *UX = W(11), *UY = W(12), *VX = W(13), *VY = W(14), *Su = W(15), *Sv = W(16);
+        T* S[6] = {W(17), W(18), W(19), W(20), W(21), W(22)};
+        T *S0 = S[0], *S1 = S[1], *S2 = S[2], *S3 = S[3], *S4 = S[4], *S5 = S[5];
+        T* zs0 = plane_t.p;                       // spectral z(0)
+        T* zx0 = plane_t.p + (size_t)M * n2;      // d/dx z(0)
+        T* zy0 = plane_t.p + (size_t)2 * M * n2;  // d/dy z(0)
+        double* wkd = plane_d.p;
+        // wkd = c2g2 * <A>
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            double s = 0.0;
+            for (int iz = 0; iz < L; iz++) s += wgt[iz] * (double)AA[(size_t)(m * L + iz) * n2 + i];
+            wkd[c] = s * c2g2[i];
+        });
+        // q and delta in physical space
+        fft.spctop(st, 2 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / ML, q = o - which * ML;
+                return (T)(which == 0 ? QS : DS)[(size_t)q * n2 + kx + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / ML, q = o - which * ML;
+                (which == 0 ? Q : DD)[(size_t)q * n2 + iy + ng * ix] = val;
+            });
+        // F = deal(ri * dpn) spectral; spectral u, v; spectral z(0)
+        fft.ptospc(st, 3 * ML + M,
+            [=] __device__(int o, int iy, int ix) -> T {
+                if (o >= 3 * ML) return Z[(size_t)((o - 3 * ML) * L) * n2 + iy + ng * ix];
+                const int which = o / ML, q = o - which * ML;
+                const size_t p = (size_t)q * n2 + iy + ng * ix;
+                return which == 0 ? RI[p] * DPN[p] : which == 1 ? U[p] : V[p];
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                if (o >= 3 * ML) { zs0[(size_t)(o - 3 * ML) * n2 + i] = val; return; }
+                const int which = o / ML, q = o - which * ML;
+                if (which == 0) F[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+                else (which == 1 ? Su : Sv)[(size_t)q * n2 + i] = val;
+            });
+        // ff, ffx, ffy, ux, uy, vx, vy, and z(0) derivatives
+        fft.spctop(st, 7 * ML + 2 * M,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+                if (o >= 7 * ML) {
+                    const int which = (o - 7 * ML) / M, m = (o - 7 * ML) % M;
+                    const T* s = zs0 + (size_t)m * n2;
+                    return which == 0 ? (T)(dmul(kx, ng) * (double)s[mx]) : (T)(dmul(ky, ng) * (double)s[my]);
+                }
+                const int which = o / ML, q = o - which * ML;
+                const T* s = (which < 3 ? F : which < 5 ? Su : Sv) + (size_t)q * n2;
+                const int kind = which < 3 ? which : (which - 3) % 2 + 1;  // 0 value, 1 d/dx, 2 d/dy
+                if (kind == 0) return s[kx + ng * ky];
+                if (kind == 1) return (T)(dmul(kx, ng) * (double)s[mx]);
+                return (T)(dmul(ky, ng) * (double)s[my]);
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int i = iy + ng * ix;
+                if (o >= 7 * ML) {
+                    const int which = (o - 7 * ML) / M, m = (o - 7 * ML) % M;
+                    (which == 0 ? zx0 : zy0)[(size_t)m * n2 + i] = val;
+                    return;
+                }
+                const int which = o / ML, q = o - which * ML;
+                T* out = which == 0 ? FF : which == 1 ? FX : which == 2 ? FY : which == 3 ? UX : which == 4 ? UY
+                       : which == 5 ? VX : VY;
+                out[(size_t)q * n2 + i] = val;
+            });
+        // products to spectral space
+        fft.ptospc(st, 6 * ML,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int which = o / ML, q = o - which * ML, m = q / L, iz = q % L;
+                const int i = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + i;
+                switch (which) {
+                    case 0: return Q[p] * U[p];
+                    case 1: return Q[p] * V[p];
+                    case 2: {
+                        const T bx = iz == 0 ? zx0[(size_t)m * n2 + i] : ZX[p];
+                        const T by = iz == 0 ? zy0[(size_t)m * n2 + i] : ZY[p];
+                        return FX[p] * by - FY[p] * bx;
+                    }
+                    case 3: return UX[p] * VY[p] - UY[p] * VX[p];
+                    case 4: return FF[p] * ZX[p] - DD[p] * U[p];
+                    default: return FF[p] * ZY[p] - DD[p] * V[p];
+                }
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int which = o / ML, q = o - which * ML;
+                T* out = which == 0 ? S0 : which == 1 ? S1 : which == 2 ? S2 : which == 3 ? S3 : which == 4 ? S4 : S5;
+                out[(size_t)q * n2 + kx + ng * ky] = val;
+            });
+        // combine in spectral space
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L;
+            const int kx = i % ng, ky = i / ng;
+            const size_t b = (size_t)q * n2;
+            const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+            const double wka = dmul(ky, ng) * (double)S1[b + my] + dmul(kx, ng) * (double)S0[b + mx];
+            const double sq = filt[i] * ((double)S2[b + i] - wka);
+            const double wkb = dmul(ky, ng) * (double)S5[b + my] + dmul(kx, ng) * (double)S4[b + mx];
+            const double sd = filt[i] * (2.0 * (double)S3[b + i] + wkb - hlap[i] * PSp[b + i]);
+            SQS[b + i] = sq;
+            SDS[b + i] = sd;
+            SGS[b + i] = COF * sq + wkd[(size_t)m * n2 + i] - FSQ * (double)AA[b + i];
+        });
+    }
+
+    // ======================================================================
+    // diagnose (src/nhswps/mod.rs:666-711): records {max(u^2+v^2), max|zeta|,
+    // sum of level-weighted zeta^2} per member in the history buffer.
+    // ======================================================================
+    void diagnose_record() {
+        const int n2 = this->n2, L = this->L, nz = this->nz;
+        T *U = u, *V = v, *ZE = zeta;
+        double* out = diag_hist.p + (size_t)(hist_rows % hist_cap) * M * 3;
+        reduce_groups<3>(st, M, (long long)L * n2, 0x3u,
+            [=] __device__(int m, long long j) {
+                const int iz = (int)(j / n2);
+                const size_t p = (size_t)m * L * n2 + j;
+                const double uu = (double)U[p], vv = (double)V[p], ze = (double)ZE[p];
+                RedVals<3> rv;
+                rv.v[0] = uu * uu + vv * vv;
+                rv.v[1] = fabs(ze);
+                rv.v[2] = (iz == 0 || iz == nz) ? 0.5 * ze * ze : ze * ze;
+                return rv;
+            }, red_partial.p, out);
+        hist_rows++;
+    }
+    void diag_finish(const double* raw, double* out4) const {
+        const double vsumi = 1.0 / (double)(ng * ng * nz);
+        const double zrms = std::sqrt(vsumi * raw[2]);
+        out4[0] = (1.0 / 2.0) * zrms * zrms;
+        out4[1] = zrms;
+        out4[2] = raw[1];
+        out4[3] = std::sqrt(raw[0]);
+    }
+
+    // energies of savegrid (src/nhswps/mod.rs:365-410)
+    void energy(int member, double* out3) {
+        const int n2 = this->n2, L = this->L, nz = this->nz;
+        T *R = r, *U = u, *V = v, *WW = w, *Z = z;
+        reduce_groups<2>(st, M, (long long)L * n2, 0u,
+            [=] __device__(int m, long long j) {
+                const int iz = (int)(j / n2);
+                const size_t p = (size_t)m * L * n2 + j;
+                const double uu = U[p], vv = V[p], ww = WW[p], rr = R[p];
+                RedVals<2> rv;
+                if (iz == 0) rv.v[0] = 0.5 * ((1.0 + rr) * (uu * uu + vv * vv));
+                else if (iz == nz) rv.v[0] = 0.5 * ((1.0 + rr) * (uu * uu + vv * vv + ww * ww));
+                else rv.v[0] = (1.0 + rr) * (uu * uu + vv * vv + ww * ww);
+                if (iz == nz) {
+                    const double h = (1.0 / HBAR) * (double)Z[p] - 1.0;
+                    rv.v[1] = h * h;
+                } else {
+                    rv.v[1] = 0.0;
+                }
+                return rv;
+            }, red_partial.p, red_out.p);
+        double h[2];
+        SW_CUDA(cudaMemcpyAsync(h_pinned, red_out.p + 2 * member, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaStreamSynchronize(st));
+        h[0] = h_pinned[0];
+        h[1] = h_pinned[1];
+        const double gl = (2.0 * PI) / (double)ng, dz = HBAR / (double)nz, gvol = gl * gl * dz;
+        const double ekin = h[0] * ((1.0 / 2.0) * gvol * (1.0 / HBAR));
+        const double epot = (1.0 / 2.0) * (gl * gl) * CSQ * h[1];
+        out3[0] = ekin;
+        out3[1] = epot;
+        out3[2] = ekin + epot;
+    }
+
+    // ======================================================================
+    // advance (src/nhswps/advance.rs:13-279)
+    // WD(2..10): qsi, qsm, sqs, sds, nds, sgs, ngs, dsi, gsi
+    // ======================================================================
+    void advance_update(bool first) {
+        const int n2 = this->n2, L = this->L;
+        const double dt = 1.0 / (double)ng, dt4 = dt / 4.0, dt4i = 1.0 / dt4;
+        const double *diss = op.diss, *rdis = op.rdis, *fope = op.fope, *c2g2 = op.c2g2, *simp = op.simp,
+                     *wgt = op.weight;
+        double *QS = qs, *DS = ds, *GS = gs;
+        double *qsi = WD(2), *qsm = WD(3), *sqs = WD(4), *sds = WD(5), *nds = WD(6), *sgs = WD(7), *ngs = WD(8),
+               *dsi = WD(9), *gsi = WD(10);
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            const size_t cb = (size_t)m * L * n2 + i;
+            const double dis = diss[i], rd = rdis[i], fo = fope[i], cg = c2g2[i], si = simp[i];
+            double wka = 0.0, wkb = 0.0;
+            for (int iz = 0; iz < L; iz++) {
+                const size_t p = cb + (size_t)iz * n2;
+                if (first) {
+                    qsi[p] = QS[p];
+                    qsm[p] = QS[p] + dt4 * sqs[p];
+                    dsi[p] = DS[p];
+                    gsi[p] = GS[p];
+                    nds[p] = sds[p] + dt4i * dsi[p];
+                    ngs[p] = sgs[p] + dt4i * gsi[p];
+                }
+                QS[p] = dis * (qsm[p] + dt4 * sqs[p]) - qsi[p];
+                const double sd = sds[p] + nds[p];
+                const double sg = sgs[p] + ngs[p];
+                sds[p] = sd;
+                sgs[p] = sg;
+                const double d = sg + rd * sd;
+                DS[p] = d;
+                wka += wgt[iz] * d;
+                wkb += wgt[iz] * sd;
+            }
+            wka *= fo;
+            wkb *= cg;
+            double wkg = 0.0;
+            for (int iz = 0; iz < L; iz++) {
+                const size_t p = cb + (size_t)iz * n2;
+                DS[p] = si * (DS[p] - wka) - dsi[p];
+                const double g = wkb - FSQ * sds[p] + rd * sgs[p];
+                GS[p] = g;
+                wkg += wgt[iz] * g;
+            }
+            wkg *= fo;
+            for (int iz = 0; iz < L; iz++) {
+                const size_t p = cb + (size_t)iz * n2;
+                GS[p] = si * (GS[p] - wkg) - gsi[p];
+            }
+        });
+    }
+
+    int advance(bool ggen) {
+        int it = 0;
+        double e = 0.0;
+        last_sweeps[0] = last_sweeps[1] = last_sweeps[2] = 0;
+        if (ggen) {
+            main_invert();
+            int stt = psolve(100, &it, &e);
+            last_sweeps[0] = it;
+            if (stt) return stt;
+        }
+        diagnose_record();
+        source(WD(4), WD(5), WD(7));
+        advance_update(true);
+        for (int k = 0; k < 2; k++) {
+            main_invert();
+            int stt = psolve(100, &it, &e);
+            last_sweeps[1 + k] = it;
+            if (stt) return stt;
+            source(WD(4), WD(5), WD(7));
+            advance_update(false);
+        }
+        t += 1.0 / (double)ng;
+        return SW_OK;
+    }
+};
+
+}  // namespace sw

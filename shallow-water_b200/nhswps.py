@@ -1,0 +1,307 @@
+"""The nhswps time-step path on the GPU (reference src/nhswps/).
+
+``State`` mirrors ``nhswps::State`` (src/nhswps/mod.rs:87-148).  Its 16 fields
+live on the device inside the ``Spectral`` context; reading ``state.u`` copies
+the field to a numpy array of shape (ng, ng, nz+1) (Fortran order) and
+assigning uploads.  The numerical entry points keep the reference's names and
+argument meaning; where the reference quits the process on a numerical failure
+(psolve.rs:349-366) these raise ``SwError`` with the same status.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from ._native import FIELDS, FIELD_INDEX, SwError, check, dptr, lib
+from .spectral import Spectral, flat, put
+
+HBAR = 0.4
+COF = 4.0 * np.pi
+CSQ = (2.0 * np.pi) ** 2
+
+
+class State:
+    """Device-resident ``nhswps::State`` of one member (member 0 of the context)."""
+
+    def __init__(self, spectral, t=0.0, ngsave=0, itime=0, jtime=0, ggen=False, member=0, **fields):
+        object.__setattr__(self, "spectral", spectral)
+        object.__setattr__(self, "member", member)
+        object.__setattr__(self, "ngsave", ngsave)
+        object.__setattr__(self, "itime", itime)
+        object.__setattr__(self, "jtime", jtime)
+        object.__setattr__(self, "ggen", ggen)
+        check(lib().sw_set_time(spectral.ctx, float(t)))
+        for k, v in fields.items():
+            setattr(self, k, v)
+
+    @property
+    def t(self):
+        t = ctypes.c_double()
+        check(lib().sw_get_time(self.spectral.ctx, ctypes.byref(t)))
+        return t.value
+
+    @t.setter
+    def t(self, value):
+        check(lib().sw_set_time(self.spectral.ctx, float(value)))
+
+    def get(self, name):
+        sp = self.spectral
+        out = np.zeros(sp.n3)
+        check(lib().sw_state_get(sp.ctx, FIELD_INDEX[name], self.member, dptr(out), sp.n3))
+        return out.reshape((sp.ng, sp.ng, sp.nz + 1), order="F")
+
+    def set(self, name, value):
+        sp = self.spectral
+        a = flat(value)
+        if a.size != sp.n3:
+            raise ValueError("%s needs %d values" % (name, sp.n3))
+        check(lib().sw_state_set(sp.ctx, FIELD_INDEX[name], self.member, dptr(a), sp.n3))
+
+    def __getattr__(self, name):
+        if name in FIELD_INDEX:
+            return self.get(name)
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name in FIELD_INDEX:
+            self.set(name, value)
+        elif name == "t":
+            State.t.fset(self, value)
+        else:
+            object.__setattr__(self, name, value)
+
+    def fields(self):
+        return {k: self.get(k) for k in FIELDS}
+
+
+def _n3(state):
+    return state.spectral.n3
+
+
+def vertical(state):
+    """z, zx, zy, aa, w from r, u, v, ds (src/nhswps/vertical.rs:8-143)."""
+    check(lib().sw_vertical(state.spectral.ctx))
+
+
+def coeffs(state, sigx=None, sigy=None, cpt1=None, cpt2=None):
+    """Pressure-iteration coefficients (src/nhswps/coeffs.rs:8-101)."""
+    n = _n3(state)
+    outs = [np.zeros(n) for _ in range(4)]
+    check(lib().sw_coeffs(state.spectral.ctx, *[dptr(o) for o in outs]))
+    for dst, o in zip((sigx, sigy, cpt1, cpt2), outs):
+        put(dst, o)
+    return outs
+
+
+def cpsource(state, sp0=None):
+    """Constant part of the pressure source (src/nhswps/cpsource.rs:13-261)."""
+    out = np.zeros(_n3(state))
+    check(lib().sw_cpsource(state.spectral.ctx, dptr(out)))
+    put(sp0, out)
+    return out
+
+
+def psolve(state, nitmax=100):
+    """Non-hydrostatic pressure (src/nhswps/psolve.rs:16-411).
+    Returns (sweeps, final relative change)."""
+    it = ctypes.c_int()
+    e = ctypes.c_double()
+    check(lib().sw_psolve(state.spectral.ctx, int(nitmax), ctypes.byref(it), ctypes.byref(e)))
+    return it.value, e.value
+
+
+def source(state, sqs=None, sds=None, sgs=None):
+    """Nonlinear source terms in spectral space (src/nhswps/source.rs:19-138)."""
+    n = _n3(state)
+    outs = [np.zeros(n) for _ in range(3)]
+    check(lib().sw_source(state.spectral.ctx, *[dptr(o) for o in outs]))
+    for dst, o in zip((sqs, sds, sgs), outs):
+        put(dst, o)
+    return outs
+
+
+def diagnose(state):
+    """(0.5*zrms^2, zrms, zmax, umax) of the current state (src/nhswps/mod.rs:666-711)."""
+    out = np.zeros(4)
+    check(lib().sw_diagnose(state.spectral.ctx, state.member, dptr(out)))
+    return out
+
+
+def energy(state):
+    """(ekin, epot, etot) as computed by savegrid (src/nhswps/mod.rs:365-410)."""
+    out = np.zeros(3)
+    check(lib().sw_energy(state.spectral.ctx, state.member, dptr(out)))
+    return out
+
+
+def diag_history(spectral, cap=4096):
+    """Diagnostics recorded at the start of each advance step since the last call."""
+    out = np.zeros((cap, 4))
+    cnt = ctypes.c_int()
+    check(lib().sw_diag_history(spectral.ctx, dptr(out), cap, ctypes.byref(cnt)))
+    return out[: cnt.value]
+
+
+def advance(state, output=None, nsteps=1):
+    """Predictor-corrector step(s) t -> t + dt (src/nhswps/advance.rs:13-279).
+    Writes the monitor.asc line of each step to ``output`` when given."""
+    t0 = state.t
+    check(lib().sw_advance(state.spectral.ctx, int(nsteps), int(bool(state.ggen))))
+    if output is not None:
+        rows = diag_history(state.spectral)
+        dt = 1.0 / state.spectral.ng
+        for k, d in enumerate(rows[-nsteps:]):
+            output.monitor.write("%.5f %.6f %.6f %.6f %.6f\n" % (t0 + k * dt, d[0], d[1], d[2], d[3]))
+    return state
+
+
+def last_sweeps(spectral):
+    out = (ctypes.c_int * 3)()
+    check(lib().sw_last_sweeps(spectral.ctx, out))
+    return list(out)
+
+
+# ---- run driver and output (src/nhswps/mod.rs:32-85, 150-663) -----------------------
+class Output:
+    """The 14 output files of nhswps (src/nhswps/mod.rs:32-85)."""
+
+    NAMES = {
+        "ecomp": "ecomp.asc", "monitor": "monitor.asc", "spectra": "spectra.asc",
+        "d3ql": "3d/ql.r4", "d3d": "3d/d.r4", "d3g": "3d/g.r4", "d3r": "3d/r.r4", "d3w": "3d/w.r4",
+        "d3pn": "3d/pn.r4", "d2q": "2d/q.r4", "d2d": "2d/d.r4", "d2g": "2d/g.r4", "d2h": "2d/h.r4",
+        "d2zeta": "2d/zeta.r4",
+    }
+
+    def __init__(self, files):
+        self.__dict__.update(files)
+
+    @classmethod
+    def from_path(cls, path):
+        os.makedirs(os.path.join(path, "2d"), exist_ok=True)
+        os.makedirs(os.path.join(path, "3d"), exist_ok=True)
+        files = {}
+        for k, rel in cls.NAMES.items():
+            files[k] = open(os.path.join(path, rel), "w" if rel.endswith(".asc") else "wb")
+        return cls(files)
+
+    def close(self):
+        for k in self.NAMES:
+            getattr(self, k).close()
+
+
+def _append_r4(f, t, data):
+    f.write(np.float32(t).astype("<f4").tobytes())
+    f.write(np.asarray(data, dtype="<f4").reshape(-1, order="F").tobytes(order="F"))
+
+
+def savegrid(state, output):
+    """Energies, spectra and f32 snapshots at a save time (src/nhswps/mod.rs:347-663)."""
+    sp = state.spectral
+    ng, nz = sp.ng, sp.nz
+    t = state.t
+    ekin, epot, etot = energy(state)
+    output.ecomp.write("%.6f %.9f %.9f %.9f %.9f %.9f\n" % (t, 0.0, ekin, ekin, epot, etot))
+    f = {k: state.get(k) for k in ("qs", "ds", "gs", "r", "w", "pn", "z", "zeta")}
+    weight = sp.weight
+    zspec = np.zeros(ng + 1)
+    dspec = np.zeros(ng + 1)
+    gspec = np.zeros(ng + 1)
+    for iz in range(nz + 1):
+        zspec += weight[iz] * sp.spec1d(sp.ptospc(f["zeta"][:, :, iz]))
+        dspec += weight[iz] * sp.spec1d(f["ds"][:, :, iz])
+        gspec += weight[iz] * sp.spec1d(f["gs"][:, :, iz])
+    spmf = sp.spmf
+    zspec *= spmf
+    dspec *= spmf
+    gspec *= spmf
+    output.spectra.write("%.6f %d\n" % (t, sp.kmaxred))
+    alk = sp.alk
+    with np.errstate(divide="ignore"):
+        for k in range(1, sp.kmaxred + 1):
+            output.spectra.write("%.8f %.8f %.8f %.8f\n" % (alk[k - 1], np.log10(zspec[k]),
+                                                          np.log10(dspec[k] + 1.0e-32), np.log10(gspec[k] + 1.0e-32)))
+    L = nz + 1
+    for key, out in (("qs", output.d3ql), ("ds", output.d3d), ("gs", output.d3g)):
+        phys = sp.spctop3d(f[key], np.zeros((ng, ng, L), order="F"), 0, nz)
+        _append_r4(out, t, phys)
+    _append_r4(output.d3r, t, f["r"])
+    _append_r4(output.d3w, t, f["w"])
+    _append_r4(output.d3pn, t, f["pn"])
+    zt = f["z"][:, :, nz]
+    _append_r4(output.d2d, t, -f["w"][:, :, nz] / zt)
+    wkp = np.zeros((ng, ng), order="F")
+    for iz in range(L):
+        wkp += weight[iz] * f["zeta"][:, :, iz] * (1.0 + f["r"][:, :, iz])
+    wkp *= HBAR / zt
+    _append_r4(output.d2zeta, t, wkp)
+    _append_r4(output.d2q, t, HBAR * (wkp + COF) / zt - COF)
+    gphys = sp.spctop3d(f["gs"], np.zeros((ng, ng, L), order="F"), 0, nz)
+    wkp = np.zeros((ng, ng), order="F")
+    for iz in range(L):
+        wkp += weight[iz] * gphys[:, :, iz] * (1.0 + f["r"][:, :, iz])
+    wkp *= HBAR / zt
+    _append_r4(output.d2g, t, wkp)
+    _append_r4(output.d2h, t, (1.0 / HBAR) * zt - 1.0)
+
+
+def _round_half_away(x):
+    """Rust's f64::round (half away from zero)."""
+    return int(np.floor(abs(x) + 0.5)) * (1 if x >= 0 else -1)
+
+
+def initial_state(spectral, qq, dd, gg):
+    """The start-up of nhswps (src/nhswps/mod.rs:238-285): physical initial
+    fields (ng*ng*(nz+1) each) -> filtered spectral qs, ds, gs with zero mean,
+    then main_invert."""
+    sp = spectral
+    ng, nz = sp.ng, sp.nz
+    st = State(sp)
+    filt = flat(sp.filt)
+    for name, src in (("qs", qq), ("ds", dd), ("gs", gg)):
+        fs = sp.ptospc3d(flat(src), np.zeros(sp.n3), 0, nz).reshape(nz + 1, ng * ng)
+        fs[:, 0] = 0.0
+        fs *= filt[None, :]
+        st.set(name, fs.reshape(-1))
+    check(lib().sw_main_invert(sp.ctx))
+    return st
+
+
+def _read_r8(path):
+    raw = np.fromfile(path, dtype="<f8")
+    return raw[1:]
+
+
+def nhswps(parameters, precision=0, device=0):
+    """Run nhswps from qq/dd/gg_init.r8 in the output directory (src/nhswps/mod.rs:150-345)."""
+    num = parameters.numerical
+    ng, nz = num.grid_resolution, num.vertical_layers
+    dt, tgsave, tsim = num.time_step, num.save_interval, num.duration
+    out_dir = str(parameters.environment.output_directory)
+    qq = _read_r8(os.path.join(out_dir, "qq_init.r8"))
+    dd = _read_r8(os.path.join(out_dir, "dd_init.r8"))
+    gg = _read_r8(os.path.join(out_dir, "gg_init.r8"))
+    sp = Spectral(ng, nz, precision=precision, device=device)
+    state = initial_state(sp, qq, dd, gg)
+    output = Output.from_path(out_dir)
+    try:
+        state.ngsave = _round_half_away(tgsave / dt)
+        while state.t <= tsim:
+            state.itime = _round_half_away(state.t / dt)
+            state.jtime = state.itime // state.ngsave
+            if state.ngsave * state.jtime == state.itime:
+                check(lib().sw_main_invert(sp.ctx))
+                psolve(state)
+                savegrid(state, output)
+                state.ggen = False
+            else:
+                state.ggen = True
+            advance(state, output)
+        state.itime = int(state.t / dt)
+        state.jtime = state.itime // state.ngsave
+        if state.ngsave * state.jtime == state.itime:
+            check(lib().sw_main_invert(sp.ctx))
+            psolve(state)
+            savegrid(state, output)
+    finally:
+        output.close()
+    return state

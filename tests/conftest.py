@@ -14,6 +14,22 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: test needs a CUDA device (B200)")
 
 
+PKG_DIR = os.path.join(ROOT, "shallow-water_b200")
+
+
+def load_package():
+    """Import the shallow-water_b200 directory as the package ``shallow_water_b200``."""
+    import importlib.util
+    if "shallow_water_b200" in sys.modules:
+        return sys.modules["shallow_water_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "shallow_water_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["shallow_water_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 _cache = {}
 
 
@@ -29,3 +45,8 @@ def oracle():
     from oracle import oracle as orc
     orc.lib()
     return orc
+
+
+@pytest.fixture(scope="session")
+def sw():
+    return load_package()

@@ -1,0 +1,222 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's golden
+vectors and the CPU oracle.
+
+Tolerances: the reference's own (1e-10 absolute for the spectral and nhswps
+functions, 1e-13 for transforms and slices, scaled by the fixture's magnitude
+where the reference compares bit-exactly), and rel-L2 <= 1e-12 against the FP64
+oracle for multi-step runs (the FP64 GPU path's stated tolerance).
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+FIELDS = ["u", "v", "w", "z", "zx", "zy", "r", "ri", "aa", "zeta", "pn", "dpn", "ps", "qs", "ds", "gs"]
+
+
+def _close(a, b, tol):
+    a = np.ravel(np.asarray(a), order="F")
+    b = np.ravel(np.asarray(b), order="F")
+    err = np.abs(a - b).max()
+    assert err <= tol, "max abs err %.3e > %.1e" % (err, tol)
+
+
+def _rel(a, b, tol=1e-13):
+    scale = max(np.abs(b).max(), 1e-300)
+    _close(np.asarray(a) / scale, np.asarray(b) / scale, tol)
+
+
+def rel_l2(a, b):
+    a = np.ravel(a, order="F")
+    b = np.ravel(b, order="F")
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+# ---- stafft / sta2dfft --------------------------------------------------------
+@pytest.mark.parametrize("n,s", [(n, s) for n in (12, 15, 16, 18, 24) for s in (1, 2)])
+def test_forfft_revfft_golden(sw, n, s):
+    g = golden("stafft")
+    _, trig = sw.stafft.initfft(n)
+    fac = sw.stafft.factorisen(n)
+    x = g["forfft/forfft_ng%d_%d_x.bin" % (n, s)].copy()
+    _rel(sw.stafft.forfft(n, n, x, trig, fac), g["forfft/forfft_ng%d_%d_x2.bin" % (n, s)])
+    x = g["revfft/revfft_ng%d_%d_x.bin" % (n, s)].copy()
+    _rel(sw.stafft.revfft(n, n, x, trig, fac), g["revfft/revfft_ng%d_%d_x2.bin" % (n, s)])
+
+
+@pytest.mark.parametrize("n", [32, 96, 160, 256, 384, 512])
+def test_fft_config_sizes_vs_oracle(sw, oracle, n):
+    """Batch (nz+1)*n = 17n columns, N(0,1) inputs (seed 2)."""
+    m = 17 * n
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(m * n)
+    ref = oracle.forfft(m, n, x)
+    got = sw.stafft.forfft(m, n, x.copy())
+    _rel(got, ref, 1e-14 * np.sqrt(n))
+    back = sw.stafft.revfft(m, n, got.copy())
+    _rel(back, x, 1e-14 * np.sqrt(n))
+
+
+def test_ptospc_spctop_golden(sw):
+    g = golden("sta2dfft")
+    sp = sw.Spectral(32, 4)
+    _rel(sp.ptospc(g["ptospc/ptospc_ng32_rvar.bin"]), g["ptospc/ptospc_ng32_svar2.bin"])
+    _rel(sp.spctop(g["spctop/spctop_ng32_svar.bin"]), g["spctop/spctop_ng32_rvar2.bin"])
+
+
+@pytest.mark.parametrize("which,case,ng", [("x", 1, 32), ("x", 2, 24), ("y", 1, 32), ("y", 2, 24)])
+def test_deriv_golden(sw, which, case, ng):
+    g = golden("sta2dfft")
+    sp = sw.Spectral(ng, 4)
+    var = g["deriv/%sderiv_%d_var.bin" % (which, case)]
+    out = sp.xderiv(var) if which == "x" else sp.yderiv(var)
+    _close(out, g["deriv/%sderiv_%d_der2.bin" % (which, case)], 0.0)
+
+
+@pytest.mark.parametrize("name", ["hlap", "glap", "rlap", "helm", "c2g2", "simp", "rope", "fope", "filt",
+                                  "diss", "opak", "rdis", "etdv", "htdv", "ap", "etd1", "htd1", "theta",
+                                  "weight", "hrkx", "hrky", "rk", "spmf"])
+def test_init_spectral_golden(sw, name):
+    sp = sw.Spectral(32, 4)
+    ref = golden("spectral")["init_spectral/32_4_%s.bin" % name]
+    _rel(np.ravel(getattr(sp, name), order="F"), ref, 1e-15)
+
+
+# ---- spectral ---------------------------------------------------------------------
+@pytest.mark.parametrize("ng,nz", [(18, 2), (30, 4), (48, 6)])
+def test_main_invert_golden(sw, ng, nz):
+    g = golden("spectral")
+    k = "main_invert/%d_%d_" % (ng, nz)
+    sp = sw.Spectral(ng, nz)
+    r, u, v, zeta = sp.main_invert(g[k + "qs.bin"], g[k + "ds.bin"], g[k + "gs.bin"])
+    for name, got in (("r", r), ("u", u), ("v", v), ("zeta", zeta)):
+        _close(got, g[k + name + ".bin"], 1e-10)
+
+
+@pytest.mark.parametrize("fn", ["jacob", "divs"])
+@pytest.mark.parametrize("ng,nz", [(30, 4), (48, 6)])
+def test_jacob_divs_golden(sw, fn, ng, nz):
+    g = golden("spectral")
+    k = "%s/%d_%d_" % (fn, ng, nz)
+    sp = sw.Spectral(ng, nz)
+    _close(getattr(sp, fn)(g[k + "aa.bin"], g[k + "bb.bin"]), g[k + "cs.bin"], 1e-10)
+
+
+@pytest.mark.parametrize("ng,nz", [(18, 2), (30, 4)])
+def test_ptospc3d_spctop3d_deal3d_golden(sw, ng, nz):
+    g = golden("spectral")
+    sp = sw.Spectral(ng, nz)
+    k = "ptospc3d/%d_%d_" % (ng, nz)
+    _close(sp.ptospc3d(g[k + "fp.bin"], g[k + "fs.bin"].copy(), 0, nz - 1), g[k + "fs2.bin"], 1e-10)
+    k = "spctop3d/%d_%d_" % (ng, nz)
+    _close(sp.spctop3d(g[k + "fs.bin"], g[k + "fp.bin"].copy(), 0, nz - 1), g[k + "fp2.bin"], 1e-10)
+    k = "deal3d/%d_%d_" % (ng, nz)
+    _close(sp.deal3d(g[k + "fp.bin"].copy()), g[k + "fp2.bin"], 1e-10)
+
+
+@pytest.mark.parametrize("ng,nz", [(18, 2), (32, 4)])
+def test_deal2d_golden(sw, ng, nz):
+    g = golden("spectral")
+    k = "deal2d/%d_%d_" % (ng, nz)
+    _close(sw.Spectral(ng, nz).deal2d(g[k + "fp.bin"].copy()), g[k + "fp2.bin"], 1e-10)
+
+
+@pytest.mark.parametrize("ng,nz", [(18, 2), (48, 4)])
+def test_spec1d_golden(sw, ng, nz):
+    g = golden("spectral")
+    k = "spec1d/%d_%d_" % (ng, nz)
+    sp = sw.Spectral(ng, nz)
+    spec = sp.spec1d(g[k + "ss.bin"])
+    _close(spec[: sp.kmax + 1], g[k + "spec2.bin"][: sp.kmax + 1], 1e-13)
+
+
+# ---- nhswps -------------------------------------------------------------------------
+def gpu_state(sw, group, case, ng, nz, t=0.0):
+    g = golden("nhswps")
+    sp = sw.Spectral(ng, nz)
+    fields = {}
+    for name in FIELDS:
+        for key in ("%s/%s_%s.bin" % (group, case, name), "%s/%s/%s.bin" % (group, case, name)):
+            if key in g:
+                fields[name] = g[key]
+    return sw.State(sp, t=t, **fields)
+
+
+def expect(group, case, name):
+    g = golden("nhswps")
+    for key in ("%s/%s_%s2.bin" % (group, case, name), "%s/%s/%s2.bin" % (group, case, name)):
+        if key in g:
+            return g[key]
+    raise KeyError(name)
+
+
+@pytest.mark.parametrize("ng,nz", [(18, 2), (32, 4)])
+def test_vertical_golden(sw, ng, nz):
+    st = gpu_state(sw, "vertical", "%d_%d" % (ng, nz), ng, nz)
+    sw.nhswps.vertical(st)
+    for name in ("z", "zx", "zy", "w", "aa"):
+        _close(st.get(name), expect("vertical", "%d_%d" % (ng, nz), name), 1e-10)
+
+
+@pytest.mark.parametrize("ng,nz", [(18, 2), (32, 4)])
+def test_coeffs_golden(sw, ng, nz):
+    case = "%d_%d" % (ng, nz)
+    st = gpu_state(sw, "coeffs", case, ng, nz)
+    outs = sw.nhswps.coeffs(st)
+    g = golden("nhswps")
+    for name, got in zip(("sigx", "sigy", "cpt1", "cpt2"), outs):
+        _close(got, g["coeffs/%s_%s2.bin" % (case, name)], 1e-10)
+
+
+@pytest.mark.parametrize("ng,nz", [(18, 2), (32, 4)])
+def test_cpsource_golden(sw, ng, nz):
+    case = "%d_%d" % (ng, nz)
+    st = gpu_state(sw, "cpsource", case, ng, nz)
+    _close(sw.nhswps.cpsource(st), golden("nhswps")["cpsource/%s_sp02.bin" % case], 1e-12)
+
+
+@pytest.mark.parametrize("ng,nz", [(18, 2), (32, 4)])
+def test_source_golden(sw, ng, nz):
+    case = "%d_%d" % (ng, nz)
+    st = gpu_state(sw, "source", case, ng, nz)
+    outs = sw.nhswps.source(st)
+    g = golden("nhswps")
+    for name, got in zip(("sqs", "sds", "sgs"), outs):
+        ref = g["source/%s_%s2.bin" % (case, name)]
+        _close(got, ref, 1e-13 * max(1.0, np.abs(ref).max()))
+
+
+@pytest.mark.parametrize("ng,nz", [(24, 4), (32, 4)])
+def test_psolve_golden(sw, oracle, ng, nz):
+    case = "%d_%d" % (ng, nz)
+    st = gpu_state(sw, "psolve", case, ng, nz)
+    it, errp = sw.nhswps.psolve(st)
+    ost = oracle.State(ng, nz, {k: np.ravel(st.get(k), order="F") for k in FIELDS})
+    # same sweep count as the oracle on the same input
+    ost2 = oracle.State(ng, nz, {k: v for k, v in _inputs("psolve", case).items()})
+    status, oit, oerr = oracle.psolve(oracle.Spectral(ng, nz), ost2)
+    assert status == 0 and it == oit
+    for name in ("z", "zx", "zy", "w", "aa", "ri", "pn", "ps", "dpn"):
+        _close(st.get(name), expect("psolve", case, name), 1e-10)
+
+
+def _inputs(group, case):
+    g = golden("nhswps")
+    out = {}
+    for name in FIELDS:
+        for key in ("%s/%s_%s.bin" % (group, case, name), "%s/%s/%s.bin" % (group, case, name)):
+            if key in g:
+                out[name] = g[key]
+    return out
+
+
+@pytest.mark.parametrize("ng,nz,t0", [(18, 6, 5.555_555_555_555_555E-2), (24, 4, 0.624_999_999_999_999_9)])
+def test_advance_golden(sw, ng, nz, t0):
+    case = "%d_%d" % (ng, nz)
+    st = gpu_state(sw, "advance", case, ng, nz, t=t0)
+    st.ggen = True
+    sw.nhswps.advance(st)
+    for name in FIELDS:
+        _close(st.get(name), expect("advance", case, name), 1e-10)
+    assert abs(st.t - (t0 + 1.0 / ng)) < 1e-12
