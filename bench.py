@@ -153,6 +153,40 @@ def run_reference(args, rank, world):
     return 0
 
 
+def time_fft_pass(sw, sp, planes, w_fft, reps=20):
+    """Average duration of one batched 2-D transform pass over `planes` planes,
+    CUDA events on the library's stream; returns (seconds per launch, bytes per launch)."""
+    import torch
+    L = sw._native.lib()
+    stream_ptr = ctypes.c_void_p()
+    sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+    dt = torch.float64 if w_fft == 8 else torch.float32
+    fbuf = torch.randn(planes * NG * NG, dtype=dt, device="cuda")
+    obuf = torch.empty_like(fbuf)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        sw._native.check(L.sw_fft2d_dev(sp.ctx, 0, planes, ctypes.c_void_p(fbuf.data_ptr()), ctypes.c_void_p(obuf.data_ptr())))
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for r in range(reps):
+        d = r & 1
+        src, dst = (fbuf, obuf) if d == 0 else (obuf, fbuf)
+        sw._native.check(L.sw_fft2d_dev(sp.ctx, d, planes, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
+    k1.record(stream)
+    torch.cuda.synchronize()
+    per_launch_s = k0.elapsed_time(k1) / 1e3 / (2 * reps)
+    return per_launch_s, 2 * planes * NG * NG * w_fft
+
+
+def fft_only(sw, sp, args, w_fft):
+    per, nbytes = time_fft_pass(sw, sp, args.planes, w_fft, reps=args.steps)
+    peak, kind = measured_peak()
+    print(json.dumps({"fft_pass_us": per * 1e6, "bytes_per_launch": nbytes, "gbs": nbytes / per / 1e9,
+                      "frac": nbytes / per / 1e9 / peak, "planes": args.planes, "precision": args.precision}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -161,6 +195,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fft-only", action="store_true",
+                    help="only time the batched 2-D transform pass (for profiling the top kernel)")
+    ap.add_argument("--planes", type=int, default=6 * (NZ + 1))
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -181,6 +218,8 @@ def main():
     w_fft = 8 if prec == sw.SW_FP64 else 4
 
     sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+    if args.fft_only:
+        return fft_only(sw, sp, args, w_fft)
     q3, d3, g3 = initial_fields(NG, NZ, 1 + rank, sw.vstrip.pv_strip)
     st = sw.nhswps.initial_state(sp, q3, d3, g3)
     stream_ptr = ctypes.c_void_p()
@@ -252,22 +291,7 @@ def main():
     # ---- dominant kernel: batched 2-D transform pass, timed live ---------------------
     peak, peak_kind = measured_peak()
     planes = 6 * (NZ + 1)
-    fbuf = torch.randn(planes * NG * NG, dtype=torch.float64 if w_fft == 8 else torch.float32, device="cuda")
-    obuf = torch.empty_like(fbuf)
-    torch.cuda.synchronize()
-    reps = 20
-    for _ in range(3):
-        sw._native.check(L.sw_fft2d_dev(sp.ctx, 0, planes, ctypes.c_void_p(fbuf.data_ptr()), ctypes.c_void_p(obuf.data_ptr())))
-    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k0.record(stream)
-    for r in range(reps):
-        d = r & 1
-        src, dst = (fbuf, obuf) if d == 0 else (obuf, fbuf)
-        sw._native.check(L.sw_fft2d_dev(sp.ctx, d, planes, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
-    k1.record(stream)
-    torch.cuda.synchronize()
-    per_launch_s = k0.elapsed_time(k1) / 1e3 / (2 * reps)
-    bytes_per_launch = 2 * planes * NG * NG * w_fft
+    per_launch_s, bytes_per_launch = time_fft_pass(sw, sp, planes, w_fft)
     achieved = bytes_per_launch / per_launch_s / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "fft_pass_traffic.json")

@@ -114,6 +114,10 @@ int sw_source(sw_ctx* ctx, double* sqs, double* sds, double* sgs);
  * ggen != 0 runs main_invert + psolve at the start of the first step (the
  * reference's State::ggen); later steps always do. */
 int sw_advance(sw_ctx* ctx, int nsteps, int ggen);
+/* Run each advance step as one CUDA graph whose pressure iterations are
+ * conditional WHILE nodes (enable = 1, the default), or drive the iterations from
+ * the host with one synchronisation per sweep (enable = 0).  Same results. */
+int sw_set_graphs(sw_ctx* ctx, int enable);
 /* diagnose (src/nhswps/mod.rs:666-711) of one member:
  * out = {0.5*zrms^2, zrms, zmax, umax}. */
 int sw_diagnose(sw_ctx* ctx, int member, double out[4]);

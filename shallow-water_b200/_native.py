@@ -63,6 +63,7 @@ _SIGS = {
     "sw_psolve": (_i, [_vp, _i, _ip, _dp]),
     "sw_source": (_i, [_vp, _dp, _dp, _dp]),
     "sw_advance": (_i, [_vp, _i, _i]),
+    "sw_set_graphs": (_i, [_vp, _i]),
     "sw_diagnose": (_i, [_vp, _i, _dp]),
     "sw_diag_history": (_i, [_vp, _dp, _i, _ip]),
     "sw_energy": (_i, [_vp, _i, _dp]),

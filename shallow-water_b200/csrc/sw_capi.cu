@@ -589,23 +589,18 @@ int sw_source(sw_ctx* ctx, double* sqs, double* sds, double* sgs) {
 int sw_advance(sw_ctx* ctx, int nsteps, int ggen) {
     return with_solver(ctx, [&](auto& s) {
         require(nsteps >= 0, SW_ERR_ARG, "nsteps must be >= 0");
-        for (int k = 0; k < nsteps; k++) {
-            int st = s.advance(k == 0 ? ggen != 0 : true);
-            if (st == SW_ERR_PSOLVE_DIVERGED) return fail(st, "Pressure error too large!");
-            if (st == SW_ERR_PSOLVE_MAXITER) return fail(st, "Exceeded maximum number of iterations to find pressure!");
-            if (st) return st;
-        }
-        return SW_OK;
+        int st = s.advance(nsteps, ggen != 0);
+        if (st == SW_ERR_PSOLVE_DIVERGED) return fail(st, "Pressure error too large!");
+        if (st == SW_ERR_PSOLVE_MAXITER) return fail(st, "Exceeded maximum number of iterations to find pressure!");
+        return st;
     });
 }
 int sw_diagnose(sw_ctx* ctx, int member, double out[4]) {
     return with_solver(ctx, [&](auto& s) {
         require(member >= 0 && member < s.M && out, SW_ERR_ARG, "bad member");
-        s.diagnose_record();
-        s.hist_rows--;
-        const double* row = s.diag_hist.p + (size_t)(s.hist_rows % s.hist_cap) * s.M * 3 + 3 * member;
+        s.diagnose_reduce();
         double raw[3];
-        SW_CUDA(cudaMemcpyAsync(s.h_pinned, row, sizeof(raw), cudaMemcpyDeviceToHost, s.st));
+        SW_CUDA(cudaMemcpyAsync(s.h_pinned, s.red_out.p + 3 * member, sizeof(raw), cudaMemcpyDeviceToHost, s.st));
         SW_CUDA(cudaStreamSynchronize(s.st));
         std::memcpy(raw, s.h_pinned, sizeof(raw));
         s.diag_finish(raw, out);
@@ -615,17 +610,19 @@ int sw_diagnose(sw_ctx* ctx, int member, double out[4]) {
 int sw_diag_history(sw_ctx* ctx, double* out, int cap, int* count) {
     return with_solver(ctx, [&](auto& s) {
         require(out && count && cap >= 0, SW_ERR_ARG, "bad arguments");
-        const int rows = std::min(std::min(s.hist_rows, s.hist_cap), cap);
-        const int first = s.hist_rows - rows;
-        std::vector<double> raw((size_t)s.hist_cap * s.M * 3);
+        int recorded = 0;
         SW_CUDA(cudaStreamSynchronize(s.st));
+        SW_CUDA(cudaMemcpy(&recorded, s.hist_dev.p, sizeof(int), cudaMemcpyDeviceToHost));
+        const int rows = std::min(std::min(recorded, s.hist_cap), cap);
+        const int first = recorded - rows;
+        std::vector<double> raw((size_t)s.hist_cap * s.M * 3);
         SW_CUDA(cudaMemcpy(raw.data(), s.diag_hist.p, raw.size() * sizeof(double), cudaMemcpyDeviceToHost));
         for (int k = 0; k < rows; k++) {
             const double* r = raw.data() + (size_t)((first + k) % s.hist_cap) * s.M * 3;
             s.diag_finish(r, out + 4 * (size_t)k);
         }
         *count = rows;
-        s.hist_rows = 0;
+        SW_CUDA(cudaMemset(s.hist_dev.p, 0, sizeof(int)));
         return SW_OK;
     });
 }
@@ -667,6 +664,12 @@ int sw_stream(sw_ctx* ctx, void** stream) {
     return with_solver(ctx, [&](auto& s) {
         require(stream != nullptr, SW_ERR_ARG, "null output");
         *stream = (void*)s.st;
+        return SW_OK;
+    });
+}
+int sw_set_graphs(sw_ctx* ctx, int enable) {
+    return with_solver(ctx, [&](auto& s) {
+        s.use_graphs = enable != 0;
         return SW_OK;
     });
 }

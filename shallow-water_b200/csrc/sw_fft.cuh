@@ -30,11 +30,34 @@ template <> struct C2<float> { using t = float2; };
 constexpr int FFT_MAX_RAD = 24;
 constexpr int FFT_THREADS = 256;
 
+// Exact quotient x / d for x, d < 2^16 by multiply-high with m = ceil(2^32 / d).
+struct FastDiv {
+    uint32_t d, m;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f;
+    f.d = d;
+    f.m = (uint32_t)((((uint64_t)1 << 32) + d - 1) / d);
+    return f;
+}
+__device__ __forceinline__ uint32_t fdiv(uint32_t x, FastDiv f) { return f.d == 1 ? x : __umulhi(x, f.m); }
+
+struct FftStage {
+    int R, Ns, nR, tstride;
+    FastDiv dNs, dnR;
+};
+
 struct FftPlan {
     int n;
     int nrad;
     int rad[FFT_MAX_RAD];
+    FftStage stg[FFT_MAX_RAD];
 };
+
+// Shared-memory index of element i of a sequence: one pad slot per 16 entries
+// keeps the strided stores of the first radix-8/16 stage free of bank conflicts.
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+__host__ __device__ inline int padded_len(int n) { return n + (n >> 4) + 1; }
 
 template <typename T2>
 __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
@@ -44,7 +67,38 @@ __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
     return r;
 }
 
-// In-register DFT of size R, sign -1 (forward) or +1 (INV).
+// v * exp(s 2 pi i j / 16), s = -1 forward, +1 inverse; j is a compile-time constant.
+template <int J, bool INV, typename T2>
+__device__ __forceinline__ T2 tw16(T2 v) {
+    using T = decltype(v.x);
+    constexpr int j = J & 15;
+    if constexpr (j == 0) return v;
+    // cos and sin of 2 pi j / 16 for j = 0..15
+    constexpr double C[16] = {1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173,
+                              0.0, -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613,
+                              -1.0, -0.92387953251128675613, -0.70710678118654752440, -0.38268343236508977173,
+                              0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613};
+    constexpr double S[16] = {0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613,
+                              1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173,
+                              0.0, -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613,
+                              -1.0, -0.92387953251128675613, -0.70710678118654752440, -0.38268343236508977173};
+    const T c = (T)C[j];
+    const T sn = INV ? (T)S[j] : (T)(-S[j]);
+    T2 r;
+    if constexpr (j == 4) {  // multiply by s*i
+        r.x = -sn * v.y; r.y = sn * v.x;
+    } else if constexpr (j == 8) {
+        r.x = -v.x; r.y = -v.y;
+    } else if constexpr (j == 12) {
+        r.x = -sn * v.y; r.y = sn * v.x;
+    } else {
+        r.x = v.x * c - v.y * sn;
+        r.y = v.x * sn + v.y * c;
+    }
+    return r;
+}
+
+// In-register DFT of size R, sign -1 (forward) or +1 (INV), natural order in/out.
 template <int R, bool INV, typename T2>
 __device__ __forceinline__ void butterfly(T2* v) {
     using T = decltype(v[0].x);
@@ -71,7 +125,7 @@ __device__ __forceinline__ void butterfly(T2* v) {
         v[0].x = v[0].x + tr; v[0].y = v[0].y + ti;
         v[1].x = mr - di; v[1].y = mi + dr;
         v[2].x = mr + di; v[2].y = mi - dr;
-    } else {  // R == 5
+    } else if constexpr (R == 5) {
         const T c51 = T(0.30901699437494742410), c52 = T(-0.80901699437494742410);
         const T s51 = T(0.95105651629515357212), s52 = T(0.58778525229247312917);
         T a1r = v[1].x + v[4].x, a1i = v[1].y + v[4].y;
@@ -87,56 +141,90 @@ __device__ __forceinline__ void butterfly(T2* v) {
         v[4].x = p1r + q1i; v[4].y = p1i - q1r;
         v[2].x = p2r - q2i; v[2].y = p2i + q2r;
         v[3].x = p2r + q2i; v[3].y = p2i - q2r;
+    } else if constexpr (R == 8) {
+        // radix-2 decimation in frequency, then two DFT-4
+        T2 a[4], b[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            a[k].x = v[k].x + v[k + 4].x; a[k].y = v[k].y + v[k + 4].y;
+            b[k].x = v[k].x - v[k + 4].x; b[k].y = v[k].y - v[k + 4].y;
+        }
+        b[1] = tw16<2, INV>(b[1]);
+        b[2] = tw16<4, INV>(b[2]);
+        b[3] = tw16<6, INV>(b[3]);
+        butterfly<4, INV>(a);
+        butterfly<4, INV>(b);
+#pragma unroll
+        for (int m = 0; m < 4; m++) { v[2 * m] = a[m]; v[2 * m + 1] = b[m]; }
+    } else {  // R == 16: X[q + 4m] = sum_k W4^{km} W16^{kq} sum_p v[k + 4p] W4^{pq}
+        T2 g[4][4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+#pragma unroll
+            for (int p = 0; p < 4; p++) g[k][p] = v[k + 4 * p];
+            butterfly<4, INV>(g[k]);
+        }
+        g[1][1] = tw16<1, INV>(g[1][1]); g[1][2] = tw16<2, INV>(g[1][2]); g[1][3] = tw16<3, INV>(g[1][3]);
+        g[2][1] = tw16<2, INV>(g[2][1]); g[2][2] = tw16<4, INV>(g[2][2]); g[2][3] = tw16<6, INV>(g[2][3]);
+        g[3][1] = tw16<3, INV>(g[3][1]); g[3][2] = tw16<6, INV>(g[3][2]); g[3][3] = tw16<9, INV>(g[3][3]);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            T2 h[4] = {g[0][q], g[1][q], g[2][q], g[3][q]};
+            butterfly<4, INV>(h);
+#pragma unroll
+            for (int m = 0; m < 4; m++) v[q + 4 * m] = h[m];
+        }
     }
 }
 
-// One Stockham pass of radix R over np sequences of length n held at x[p*n + j].
+// One Stockham pass of radix R over np sequences (padded, stride pl) in x -> y.
 template <int R, bool INV, typename T2>
 __device__ __forceinline__ void stockham_stage(const T2* __restrict__ x, T2* __restrict__ y,
-                                               const T2* __restrict__ tw, int n, int Ns, int np) {
-    const int nR = n / R;
-    const int tstride = n / (Ns * R);
+                                               const T2* __restrict__ tw, const FftStage& sg, int np, int pl) {
+    const int nR = sg.nR;
     for (int b = threadIdx.x; b < np * nR; b += blockDim.x) {
-        const int p = b / nR;
+        const int p = (int)fdiv((uint32_t)b, sg.dnR);
         const int j = b - p * nR;
-        const int k = j % Ns;
-        const int base = (j - k) * R + k;
-        const T2* xp = x + p * n;
-        T2* yp = y + p * n;
+        const int jq = (int)fdiv((uint32_t)j, sg.dNs);
+        const int k = j - jq * sg.Ns;
+        const int base = jq * sg.Ns * R + k;
+        const T2* xp = x + p * pl;
+        T2* yp = y + p * pl;
         T2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) v[r] = xp[j + r * nR];
-        if (Ns > 1) {
+        for (int r = 0; r < R; r++) v[r] = xp[pad16(j + r * nR)];
+        if (sg.Ns > 1) {
+            const int step = k * sg.tstride;
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                T2 w = tw[r * k * tstride];
+                T2 w = tw[r * step];
                 if (INV) w.y = -w.y;
                 v[r] = cmul(v[r], w);
             }
         }
         butterfly<R, INV>(v);
 #pragma unroll
-        for (int r = 0; r < R; r++) yp[base + r * Ns] = v[r];
+        for (int r = 0; r < R; r++) yp[pad16(base + r * sg.Ns)] = v[r];
     }
 }
 
 // Full transform of np sequences; returns the buffer holding the result.
 template <bool INV, typename T2>
-__device__ T2* smem_fft(const FftPlan& plan, T2* a, T2* b, const T2* tw, int np) {
-    int Ns = 1;
+__device__ T2* smem_fft(const FftPlan& plan, T2* a, T2* b, const T2* tw, int np, int pl) {
     for (int s = 0; s < plan.nrad; s++) {
-        const int R = plan.rad[s];
-        switch (R) {
-            case 4: stockham_stage<4, INV>(a, b, tw, plan.n, Ns, np); break;
-            case 2: stockham_stage<2, INV>(a, b, tw, plan.n, Ns, np); break;
-            case 3: stockham_stage<3, INV>(a, b, tw, plan.n, Ns, np); break;
-            default: stockham_stage<5, INV>(a, b, tw, plan.n, Ns, np); break;
+        const FftStage& sg = plan.stg[s];
+        switch (sg.R) {
+            case 16: stockham_stage<16, INV>(a, b, tw, sg, np, pl); break;
+            case 8: stockham_stage<8, INV>(a, b, tw, sg, np, pl); break;
+            case 4: stockham_stage<4, INV>(a, b, tw, sg, np, pl); break;
+            case 2: stockham_stage<2, INV>(a, b, tw, sg, np, pl); break;
+            case 3: stockham_stage<3, INV>(a, b, tw, sg, np, pl); break;
+            default: stockham_stage<5, INV>(a, b, tw, sg, np, pl); break;
         }
         __syncthreads();
         T2* t = a;
         a = b;
         b = t;
-        Ns *= R;
     }
     return a;
 }
@@ -144,33 +232,55 @@ __device__ T2* smem_fft(const FftPlan& plan, T2* a, T2* b, const T2* tw, int np)
 // Shared memory bytes of one pass: twiddles (n) + two tiles (tc/2 * n each).
 template <typename T>
 inline size_t fft_pass_smem(int n, int tc) {
-    return sizeof(typename C2<T>::t) * (size_t)n * (size_t)(1 + tc);
+    return sizeof(typename C2<T>::t) * ((size_t)n + (size_t)tc * padded_len(n));
 }
 
 // Generic tile pass.  grid.x = column tiles, grid.y = output index o.
+// tc (columns per tile) is a power of two, 1 << ltc.  Loads are issued in
+// unrolled groups of FFT_UNROLL per thread so that many global reads are in
+// flight before the tile is written to shared memory.
+constexpr int FFT_UNROLL = 8;
+
 template <typename T, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
-__global__ void __launch_bounds__(FFT_THREADS)
-k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, int tc, T sc, LD ld, ST st) {
+__global__ void __launch_bounds__(FFT_THREADS, 3)
+k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, int ltc, FastDiv dn, T sc, LD ld, ST st) {
     using T2 = typename C2<T>::t;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = plan.n;
+    const int tc = 1 << ltc;
     const int np = tc >> 1;
+    const int pl = padded_len(n);
     T2* tw = reinterpret_cast<T2*>(smem_raw);
     T2* buf0 = tw + n;
-    T2* buf1 = buf0 + (size_t)np * n;
+    T2* buf1 = buf0 + (size_t)np * pl;
     const int o = blockIdx.y;
     const int c0 = blockIdx.x * tc;
     const int nthr = blockDim.x;
+    const int total = tc * n;
 
     for (int i = threadIdx.x; i < n; i += nthr) tw[i] = twg[i];
     T* rb = reinterpret_cast<T*>(buf0);
-    for (int idx = threadIdx.x; idx < tc * n; idx += nthr) {
-        int c, j;
-        if (LOAD_CF) { c = idx % tc; j = idx / tc; }
-        else         { j = idx % n;  c = idx / n; }
-        const int col = c0 + c;
-        T val = (col < ncols) ? (T)ld(o, col, j) : T(0);
-        rb[(((c >> 1) * n + j) << 1) + (c & 1)] = val;
+    for (int base = 0; base < total; base += nthr * FFT_UNROLL) {
+        T vals[FFT_UNROLL];
+#pragma unroll
+        for (int u = 0; u < FFT_UNROLL; u++) {
+            const int idx = base + u * nthr + threadIdx.x;
+            int c, j;
+            if (LOAD_CF) { c = idx & (tc - 1); j = idx >> ltc; }
+            else         { j = (int)((uint32_t)idx - fdiv((uint32_t)idx, dn) * (uint32_t)n); c = (int)fdiv((uint32_t)idx, dn); }
+            const int col = c0 + c;
+            vals[u] = (idx < total && col < ncols) ? (T)ld(o, col, j) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < FFT_UNROLL; u++) {
+            const int idx = base + u * nthr + threadIdx.x;
+            if (idx < total) {
+                int c, j;
+                if (LOAD_CF) { c = idx & (tc - 1); j = idx >> ltc; }
+                else         { c = (int)fdiv((uint32_t)idx, dn); j = idx - c * n; }
+                rb[(((c >> 1) * pl + pad16(j)) << 1) + (c & 1)] = vals[u];
+            }
+        }
     }
     __syncthreads();
     if (INV) {
@@ -179,32 +289,33 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
         for (int idx = threadIdx.x; idx < np * kh; idx += nthr) {
             const int p = idx / kh;
             const int k = 1 + idx - p * kh;
-            T2* z = buf0 + p * n;
-            T2 lo = z[k], hi = z[n - k];  // lo = (Ha[k], Hb[k]), hi = (Ha[n-k], Hb[n-k])
+            T2* z = buf0 + p * pl;
+            T2 lo = z[pad16(k)], hi = z[pad16(n - k)];  // lo = (Ha[k], Hb[k]), hi = (Ha[n-k], Hb[n-k])
             T2 zk, znk;
             zk.x = lo.x - hi.y;  zk.y = hi.x + lo.y;
             znk.x = lo.x + hi.y; znk.y = lo.y - hi.x;
-            z[k] = zk;
-            z[n - k] = znk;
+            z[pad16(k)] = zk;
+            z[pad16(n - k)] = znk;
         }
         __syncthreads();
     }
-    const T2* Z = smem_fft<INV>(plan, buf0, buf1, tw, np);
-    for (int idx = threadIdx.x; idx < tc * n; idx += nthr) {
+    const T2* Z = smem_fft<INV>(plan, buf0, buf1, tw, np, pl);
+    for (int idx = threadIdx.x; idx < total; idx += nthr) {
         int c, k;
-        if (STORE_CF) { c = idx % tc; k = idx / tc; }
-        else          { k = idx % n;  c = idx / n; }
+        if (STORE_CF) { c = idx & (tc - 1); k = idx >> ltc; }
+        else          { c = (int)fdiv((uint32_t)idx, dn); k = idx - c * n; }
         const int col = c0 + c;
         if (col >= ncols) continue;
-        const T2* z = Z + (c >> 1) * n;
+        const T2* z = Z + (c >> 1) * pl;
         T val;
         if (!INV) {
-            const T2 a = z[k];
-            const T2 b = z[k == 0 ? 0 : n - k];
+            const T2 a = z[pad16(k)];
+            const T2 b = z[pad16(k == 0 ? 0 : n - k)];
             if (2 * k <= n) val = (c & 1) ? T(0.5) * (a.y + b.y) : T(0.5) * (a.x + b.x);
             else            val = (c & 1) ? T(0.5) * (a.x - b.x) : T(0.5) * (b.y - a.y);
         } else {
-            val = (c & 1) ? z[k].y : z[k].x;
+            const T2 a = z[pad16(k)];
+            val = (c & 1) ? a.y : a.x;
         }
         st(o, col, k, val * sc);
     }

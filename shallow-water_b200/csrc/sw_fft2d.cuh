@@ -50,15 +50,34 @@ inline int build_plan(int n, FftPlan& plan) {
     int rem = n;
     plan.n = n;
     plan.nrad = 0;
-    if (n < 2) return SW_ERR_FACTORISE;
-    const int order[4] = {4, 2, 3, 5};
+    if (n < 2 || n > 4096) return SW_ERR_FACTORISE;
+    // largest radices first: fewer shared-memory passes (n = 256 -> 16 x 16)
+    const int order[6] = {16, 8, 4, 2, 3, 5};
     for (int r : order)
         while (rem % r == 0) {
             if (plan.nrad >= FFT_MAX_RAD) return SW_ERR_FACTORISE;
+            if (r == 16 && n == 512 && plan.nrad == 0) break;  // 512 = 8 x 8 x 8 (fewer registers than 16 x 16 x 2)
             plan.rad[plan.nrad++] = r;
             rem /= r;
         }
-    return rem == 1 ? SW_OK : SW_ERR_FACTORISE;
+    if (n == 512) {
+        plan.nrad = 3;
+        plan.rad[0] = plan.rad[1] = plan.rad[2] = 8;
+        rem = 1;
+    }
+    if (rem != 1) return SW_ERR_FACTORISE;
+    int Ns = 1;
+    for (int s = 0; s < plan.nrad; s++) {
+        FftStage& g = plan.stg[s];
+        g.R = plan.rad[s];
+        g.Ns = Ns;
+        g.nR = n / g.R;
+        g.tstride = n / (Ns * g.R);
+        g.dNs = make_fastdiv((uint32_t)Ns);
+        g.dnR = make_fastdiv((uint32_t)g.nR);
+        Ns *= g.R;
+    }
+    return SW_OK;
 }
 
 // Twiddles exp(-2 pi i t/n), t < n, computed in float64 on the host.
@@ -73,15 +92,19 @@ inline std::vector<typename C2<T>::t> host_twiddles(int n) {
     return tw;
 }
 
-// Columns per CTA: even, keeps the pass within ~72 KB of shared memory.
+// Columns per CTA: a power of two (>= 2), keeping the pass within ~76 KB of
+// shared memory so that several CTAs share an SM.
 template <typename T>
 inline int pick_tile(int n) {
-    const int budget = 72 * 1024 / (int)sizeof(typename C2<T>::t);
-    int tc = budget / n - 1;
-    if (tc > 32) tc = 32;
-    tc &= ~1;
-    if (tc < 2) tc = 2;
+    const int budget = 76 * 1024 / (int)sizeof(typename C2<T>::t) - n;
+    int tc = 2;
+    while (tc * 2 <= 32 && (tc * 2) * padded_len(n) <= budget) tc *= 2;
     return tc;
+}
+inline int ilog2(int x) {
+    int l = 0;
+    while ((1 << (l + 1)) <= x) l++;
+    return l;
 }
 
 template <typename T, bool INV, bool LCF, bool SCF, class LD, class ST>
@@ -95,10 +118,11 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
     cudaGetDevice(&dev);
     if (dev < 64 && !attr_done[dev]) {
         SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         attr_done[dev] = 1;
     }
     dim3 grid((ncols + tc - 1) / tc, nout);
-    kern<<<grid, FFT_THREADS, smem, s>>>(plan, tw, ncols, tc, sc, ld, st);
+    kern<<<grid, FFT_THREADS, smem, s>>>(plan, tw, ncols, ilog2(tc), make_fastdiv((uint32_t)plan.n), sc, ld, st);
     SW_CHECK_LAUNCH();
     count_launch();
 }

@@ -52,7 +52,15 @@ struct Solver {
     DevBuf<double> errp_d, diag_hist;
     DevBuf<int> ctrl;  // per member: active, iters, status
     double* h_pinned = nullptr;  // host staging for small readbacks
-    int hist_cap = 4096, hist_rows = 0;
+    int hist_cap = 4096;
+    // whole-step CUDA graphs (index: ggen) with device-side psolve loops
+    cudaStream_t st_body = nullptr;
+    cudaGraphExec_t step_exec[2] = {nullptr, nullptr};
+    DevBuf<int> sweeps_dev;  // per member: sweep counts of the 3 psolve calls of the last step
+    DevBuf<int> err_dev;     // sticky status of captured steps
+    DevBuf<int> hist_dev;    // diagnostics rows recorded since the last read
+    DevBuf<long long> sweep_exec;  // sweep bodies executed by graph launches (launch accounting)
+    long long k_fixed[2] = {0, 0}, k_sweep = 0;  // kernels per step outside the sweeps, per sweep
     int last_sweeps[3] = {0, 0, 0};
 
     static constexpr int NWT = 24;
@@ -95,9 +103,21 @@ struct Solver {
         diag_hist.alloc((size_t)hist_cap * M * 3);
         ctrl.alloc((size_t)3 * M + 1);
         SW_CUDA(cudaMallocHost(&h_pinned, sizeof(double) * (16 * (size_t)M + 64)));
+        SW_CUDA(cudaStreamCreateWithFlags(&st_body, cudaStreamNonBlocking));
+        sweeps_dev.alloc((size_t)3 * M);
+        err_dev.alloc(1);
+        hist_dev.alloc(1);
+        sweep_exec.alloc(1);
+        SW_CUDA(cudaMemset(sweep_exec.p, 0, sizeof(long long)));
+        SW_CUDA(cudaMemset(sweeps_dev.p, 0, sizeof(int) * 3 * M));
+        SW_CUDA(cudaMemset(err_dev.p, 0, sizeof(int)));
+        SW_CUDA(cudaMemset(hist_dev.p, 0, sizeof(int)));
     }
     ~Solver() {
         if (st) cudaStreamSynchronize(st);
+        for (auto& e : step_exec)
+            if (e) cudaGraphExecDestroy(e);
+        if (st_body) cudaStreamDestroy(st_body);
         if (h_pinned) cudaFreeHost(h_pinned);
         if (st) cudaStreamDestroy(st);
     }
@@ -192,6 +212,11 @@ struct Solver {
         const double *theta = op.theta, *filt = op.filt, *DS = ds;
         T *Z = z, *R = r, *U = u, *V = v, *WW = w, *ZX = zx, *ZY = zy, *AA = aa;
         T *S1 = W(0), *SA = W(1), *SB = W(2), *RS = W(3);
+        // float32 path: the derivatives are taken of the deviation z - theta, kept
+        // apart from z so that its float32 rounding is relative to the deviation
+        // (theta is horizontally uniform, so the derivatives are the same).
+        const bool mixed = sizeof(T) == 4;
+        T* zd = W(20);
         // z by trapezoidal integration of rho'_theta, then + theta
         for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
@@ -199,18 +224,21 @@ struct Solver {
             const T* rc = R + (size_t)m * L * n2 + i;
             double prev = dz2 * ((double)rc[0] + (double)rc[n2]);
             zc[n2] = (T)prev;
+            if (mixed) zd[(size_t)m * L * n2 + i + n2] = (T)prev;
             for (int iz = 1; iz < nz; iz++) {
                 prev = prev + dz2 * ((double)rc[(size_t)iz * n2] + (double)rc[(size_t)(iz + 1) * n2]);
                 zc[(size_t)(iz + 1) * n2] = (T)prev;
+                if (mixed) zd[(size_t)m * L * n2 + i + (size_t)(iz + 1) * n2] = (T)prev;
             }
             for (int iz = 1; iz <= nz; iz++) zc[(size_t)iz * n2] = (T)((double)zc[(size_t)iz * n2] + theta[iz]);
         });
         // z_x, z_y for iz = 1..nz
         const int Mnz = M * nz;
+        const T* zsrc = mixed ? zd : Z;
         fft.ptospc(st, Mnz,
             [=] __device__(int o, int iy, int ix) -> T {
                 const int m = o / nz, iz = 1 + o % nz;
-                return Z[(size_t)(m * L + iz) * n2 + iy + ng * ix];
+                return zsrc[(size_t)(m * L + iz) * n2 + iy + ng * ix];
             },
             [=] __device__(int o, int kx, int ky, T val) {
                 const int m = o / nz, iz = 1 + o % nz;
@@ -382,14 +410,51 @@ struct Solver {
         T *Pp = W(17), *Pq = W(18), *Pr = W(19);
         T* hs = plane_t.p;        // M planes: spectral then physical hsrc
         T* hsrc = plane_t.p + (size_t)M * n2;
+        // float32 path: -g Lap(h) and f zeta nearly cancel (geostrophic balance), so
+        // their sum is formed in float64 spectral space from qs and gs (h and zeta as
+        // main_invert defines them) and only the small residual is transformed.
+        const bool mixed = sizeof(T) == 4;
+        T* HZ = W(21);
+        if (mixed) {
+            const double *QS = qs, *GS = gs, *rope = op.rope, *wgt = op.weight;
+            const double dz2 = (HBAR / (double)nz) / 2.0;
+            double* hspec = plane_d.p;  // per member: spectral h deviation (trapezoid of rho')
+            for_cols(st, M * n2, [=] __device__(int c) {
+                const int m = c / n2, i = c - m * n2;
+                double w = 0.0;
+                for (int iz = 0; iz < L; iz++) {
+                    const size_t p = (size_t)(m * L + iz) * n2 + i;
+                    w += wgt[iz] * (COFI * (COFI * GS[p] - QS[p]));
+                }
+                w *= rope[i];
+                double h = 0.0, prev = 0.0;
+                for (int iz = 0; iz < L; iz++) {
+                    const size_t p = (size_t)(m * L + iz) * n2 + i;
+                    const double wka = COFI * (COFI * GS[p] - QS[p]) - w;
+                    if (iz > 0) h += dz2 * (prev + wka);
+                    prev = wka;
+                }
+                hspec[c] = h;
+                hspec[(size_t)M * n2 + c] = w;
+            });
+            fft.spctop(st, ML,
+                [=] __device__(int q, int kx, int ky) -> T {
+                    const int m = q / L, i = kx + ng * ky;
+                    const size_t p = (size_t)q * n2 + i;
+                    const double w = hspec[(size_t)M * n2 + (size_t)m * n2 + i];
+                    const double zeta_s = QS[p] + COF * (COFI * (COFI * GS[p] - QS[p]) - w);
+                    return (T)(glap[i] * hspec[(size_t)m * n2 + i] + COF * zeta_s);
+                },
+                [=] __device__(int q, int iy, int ix, T val) { HZ[(size_t)q * n2 + iy + ng * ix] = val; });
+        }
         // hsrc = -g Lap(h) in physical space
-        fft.ptospc(st, M,
+        if (!mixed) fft.ptospc(st, M,
             [=] __device__(int m, int iy, int ix) -> T { return Z[(size_t)(m * L + nz) * n2 + iy + ng * ix]; },
             [=] __device__(int m, int kx, int ky, T val) {
                 const int i = kx + ng * ky;
                 hs[(size_t)m * n2 + i] = (T)((double)val * glap[i]);
             });
-        fft.spctop(st, M,
+        if (!mixed) fft.spctop(st, M,
             [=] __device__(int m, int kx, int ky) -> T { return hs[(size_t)m * n2 + kx + ng * ky]; },
             [=] __device__(int m, int iy, int ix, T val) { hsrc[(size_t)m * n2 + iy + ng * ix] = val; });
         // horizontal derivatives of u, v, w
@@ -469,17 +534,28 @@ struct Solver {
                 const int m = q / L, iz = q % L;
                 const int i = iy + ng * ix;
                 const size_t p = (size_t)q * n2 + i;
-                const double hsv = (double)hsrc[(size_t)m * n2 + i];
                 const double ux = UX[p], uy = UY[p], vx = VX[p], vy = VY[p];
                 double s;
-                if (iz == 0) {
-                    const double wkq = Pq[p];
-                    s = hsv + COF * (double)ZE[p];
-                    s += 2.0 * (ux * vy - uy * vx + wkq * (ux + vy));
+                if (mixed) {
+                    const double hz = HZ[p];  // -g Lap(h) + f zeta
+                    if (iz == 0) {
+                        s = hz + 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
+                    } else {
+                        const double rip = RI[p];
+                        s = hz - COF * (rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
+                        s += 2.0 * (ux * vy - uy * vx);
+                    }
                 } else {
-                    const double rip = RI[p];
-                    s = hsv + COF * ((double)ZE[p] - rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
-                    s += 2.0 * (ux * vy - uy * vx);
+                    const double hsv = (double)hsrc[(size_t)m * n2 + i];
+                    if (iz == 0) {
+                        const double wkq = Pq[p];
+                        s = hsv + COF * (double)ZE[p];
+                        s += 2.0 * (ux * vy - uy * vx + wkq * (ux + vy));
+                    } else {
+                        const double rip = RI[p];
+                        s = hsv + COF * ((double)ZE[p] - rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
+                        s += 2.0 * (ux * vy - uy * vx);
+                    }
                 }
                 SP0[p] = (T)s;
             });
@@ -492,11 +568,16 @@ struct Solver {
     // ctrl: [active, iters, status] per member; errp_d: errp per member.
     // Returns member-0 status.
     // ======================================================================
-    int psolve(int nitmax, int* iters_out, double* errp_out) {
+    void psolve_prepare(int nitmax) {
         const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
         require(nz >= 3, SW_ERR_ARG, "psolve needs nz >= 3");
-        if (nitmax <= 0) nitmax = 100;
-        const double toler = 1.0E-9;
+        (void)nitmax;
+        // Stop rule (psolve.rs:17, 89).  float64 path: the reference's 1e-9 on the
+        // relative change.  float32 transforms put a floor of ~1e-6 under that
+        // change, so the mixed path stops at 1e-6, or earlier once the change has
+        // stagnated (< 1e-4 and no longer shrinking by 30% per sweep).
+        const bool mixed = sizeof(T) == 4;
+        const double toler = mixed ? 1.0E-6 : 1.0E-9;
         const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz2 = dz / 2.0, dz6 = dz / 6.0;
         const double dzisq = (1.0 / dz) * (1.0 / dz);
         const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
@@ -536,145 +617,204 @@ struct Solver {
             ctl[3 * m + 1] = 0;
             ctl[3 * m + 2] = SW_OK;
         });
+    }
+
+    // One pressure sweep (psolve.rs:89-358) and its convergence control.  With
+    // cond set, the sweep is the body of a graph WHILE node and the last kernel
+    // sets the node's condition from the members still iterating.
+    void psolve_sweep(int nitmax, bool use_cond, cudaGraphConditionalHandle cond) {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+        const bool mixed = sizeof(T) == 4;
+        const double toler = mixed ? 1.0E-6 : 1.0E-9;
+        const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz2 = dz / 2.0, dz6 = dz / 6.0;
+        const double dzisq = (1.0 / dz) * (1.0 / dz);
+        const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
+        const double *filt = op.filt, *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap, *htd1 = op.htd1, *etd1 = op.etd1;
+        T *R = r, *RI = ri, *PN = pn, *DPN = dpn;
+        double* PS = ps;
+        T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
+        T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
+        double* PSA = WD(0);
+        int* ctl = ctrl.p;
+        double* errp = errp_d.p;
+        (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;
+        (void)SIGX; (void)SIGY; (void)C1; (void)C2; (void)SP0; (void)A; (void)B; (void)C; (void)D; (void)ctl; (void)errp;
+        (void)htdv; (void)etdv; (void)ap; (void)dz2; (void)dzisq; (void)hdzi; (void)mixed;
         const int nsp = 4 * nz - 1;  // spctop outputs per member per sweep
-        int sweeps = 0;
-        while (true) {
             // (a) pressure derivative terms to physical space
-            fft.spctop(st, M * nsp,
-                [=] __device__(int o, int kx, int ky) -> T {
-                    const int m = o / nsp, k = o - m * nsp;
-                    const double* pc = PS + (size_t)m * L * n2 + kx + ng * ky;
-                    auto P = [&](int iz, int dx, int dy) {
-                        const int jx = dx ? mirror(kx, ng) : kx, jy = dy ? mirror(ky, ng) : ky;
-                        return pc[(size_t)iz * n2 + (jx - kx) + ng * (jy - ky)];
-                    };
-                    auto wka = [&](int iz, int dx, int dy) { return (P(iz + 1, dx, dy) - P(iz - 1, dx, dy)) * hdzi; };
-                    auto wkd = [&](int iz, int dx, int dy) {
-                        return (P(iz + 1, dx, dy) - 2.0 * P(iz, dx, dy) + P(iz - 1, dx, dy)) * dzisq;
-                    };
-                    if (k == 0) return (T)((2.0 * P(0, 0, 0) - 5.0 * P(1, 0, 0) + 4.0 * P(2, 0, 0) - P(3, 0, 0)) * dzisq);
-                    if (k < 4 * nz - 3) {
-                        const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
-                        if (kind == 0) return (T)(dmul(kx, ng) * wka(iz, 1, 0));
-                        if (kind == 1) return (T)(dmul(ky, ng) * wka(iz, 0, 1));
-                        if (kind == 2) return (T)wka(iz, 0, 0);
-                        return (T)wkd(iz, 0, 0);
-                    }
-                    // extrapolated dp/dtheta at iz = nz (spectral form of psolve.rs:232-238)
-                    const int dx = (k == 4 * nz - 3), dy = !dx;
-                    const double sa = wka(nz - 1, dx, dy) + dz2 * (3.0 * wkd(nz - 1, dx, dy) - wkd(nz - 2, dx, dy));
-                    return (T)((dx ? dmul(kx, ng) : dmul(ky, ng)) * sa);
-                },
-                [=] __device__(int o, int iy, int ix, T val) {
-                    const int m = o / nsp, k = o - m * nsp;
-                    const size_t base = (size_t)m * L * n2 + iy + ng * ix;
-                    if (k == 0) { D[base] = val; return; }
-                    if (k < 4 * nz - 3) {
-                        const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
-                        T* out = kind == 0 ? A : kind == 1 ? B : kind == 2 ? C : D;
-                        out[base + (size_t)iz * n2] = val;
-                        return;
-                    }
-                    ((k == 4 * nz - 3) ? A : B)[base + (size_t)nz * n2] = val;
-                });
-            // (b) total source S = S0 + S1(p), to spectral space
-            fft.ptospc(st, ML,
-                [=] __device__(int q, int iy, int ix) -> T {
-                    const int m = q / L, iz = q % L;
-                    const int i = iy + ng * ix;
-                    const size_t p = (size_t)q * n2 + i;
-                    const size_t cb = (size_t)m * L * n2 + i;
-                    double s;
-                    if (iz == 0) {
-                        s = (double)SP0[p] + (double)C2[p] * (double)D[p];
-                    } else if (iz < nz) {
-                        s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
-                        s += (double)C2[p] * (double)D[p] + (double)C1[p] * (double)C[p];
-                    } else {
-                        const double d1 = D[cb + (size_t)(nz - 1) * n2], d2 = D[cb + (size_t)(nz - 2) * n2];
-                        const double dpdt = (double)C[cb + (size_t)(nz - 1) * n2] + dz2 * (3.0 * d1 - d2);
-                        const double d2pdt2 = 2.0 * d1 - d2;
-                        s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
-                        s += (double)C2[p] * d2pdt2 + (double)C1[p] * dpdt;
-                    }
-                    return (T)s;
-                },
-                [=] __device__(int q, int kx, int ky, T val) { SP[(size_t)q * n2 + kx + ng * ky] = val; });
-            // (c) compact RHS and Thomas solve per (kx, ky) column; residual terms
-            double* cterm = WD(1);  // per column: [num, den] packed as two planes of M*n2
-            for_cols(st, M * n2, [=] __device__(int c) {
-                const int m = c / n2, i = c - m * n2;
-                const size_t cb = (size_t)m * L * n2 + i;
-                double* num = cterm + c;
-                double* den = cterm + (size_t)M * n2 + c;
-                if (!ctl[3 * m]) { *num = 0.0; *den = 0.0; return; }
-                double sp[MAX_NZ + 1], x[MAX_NZ + 1];
-                for (int iz = 0; iz <= nz; iz++) sp[iz] = (double)SP[cb + (size_t)iz * n2];
-                const double api = ap[i];
-                x[0] = ((1.0 / 3.0) * sp[0] + (1.0 / 6.0) * sp[1]) * htdv[i];
-                for (int iz = 1; iz < nz; iz++) {
-                    const double g = (1.0 / 12.0) * (sp[iz - 1] + sp[iz + 1]) + (5.0 / 6.0) * sp[iz];
-                    x[iz] = (g - api * x[iz - 1]) * htdv[i + (size_t)n2 * iz];
+        fft.spctop(st, M * nsp,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int m = o / nsp, k = o - m * nsp;
+                const double* pc = PS + (size_t)m * L * n2 + kx + ng * ky;
+                auto P = [&](int iz, int dx, int dy) {
+                    const int jx = dx ? mirror(kx, ng) : kx, jy = dy ? mirror(ky, ng) : ky;
+                    return pc[(size_t)iz * n2 + (jx - kx) + ng * (jy - ky)];
+                };
+                auto wka = [&](int iz, int dx, int dy) { return (P(iz + 1, dx, dy) - P(iz - 1, dx, dy)) * hdzi; };
+                auto wkd = [&](int iz, int dx, int dy) {
+                    return (P(iz + 1, dx, dy) - 2.0 * P(iz, dx, dy) + P(iz - 1, dx, dy)) * dzisq;
+                };
+                if (k == 0) return (T)((2.0 * P(0, 0, 0) - 5.0 * P(1, 0, 0) + 4.0 * P(2, 0, 0) - P(3, 0, 0)) * dzisq);
+                if (k < 4 * nz - 3) {
+                    const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
+                    if (kind == 0) return (T)(dmul(kx, ng) * wka(iz, 1, 0));
+                    if (kind == 1) return (T)(dmul(ky, ng) * wka(iz, 0, 1));
+                    if (kind == 2) return (T)wka(iz, 0, 0);
+                    return (T)wkd(iz, 0, 0);
                 }
-                for (int iz = nz - 2; iz >= 0; iz--) x[iz] += etdv[i + (size_t)n2 * iz] * x[iz + 1];
-                x[nz] = 0.0;
-                const int kx = i % ng, ky = i / ng;
-                const double wgt = pweight(kx, ng) * pweight(ky, ng);
-                double sn = 0.0, sd = 0.0;
-                for (int iz = 0; iz <= nz; iz++) {
-                    const size_t p = cb + (size_t)iz * n2;
-                    const double old = PSA[p];
-                    sn += (x[iz] - old) * (x[iz] - old);
-                    sd += old * old;
-                    PS[p] = x[iz];
-                    PSA[p] = x[iz];
-                }
-                *num = wgt * sn;
-                *den = wgt * sd;
-            });
-            reduce_groups<2>(st, M, n2, 0u,
-                [=] __device__(int g, long long i) {
-                    RedVals<2> rv;
-                    rv.v[0] = cterm[(size_t)g * n2 + i];
-                    rv.v[1] = cterm[(size_t)M * n2 + (size_t)g * n2 + i];
-                    return rv;
-                }, red_partial.p, red_out.p);
-            // (d) convergence control (psolve.rs:89, 339-358)
-            const double* sums = red_out.p;
-            for_cols(st, M, [=] __device__(int m) {
-                if (!ctl[3 * m]) return;
-                const double e = sqrt(sums[2 * m] / (sums[2 * m + 1] + 1.0E-20));
-                errp[m] = e;
-                const int it = ctl[3 * m + 1];
-                if (it > 0 && e > 1.0) {
-                    ctl[3 * m + 2] = SW_ERR_PSOLVE_DIVERGED;
-                    ctl[3 * m] = 0;
-                    ctl[3 * m + 1] = it + 1;
+                // extrapolated dp/dtheta at iz = nz (spectral form of psolve.rs:232-238)
+                const int dx = (k == 4 * nz - 3), dy = !dx;
+                const double sa = wka(nz - 1, dx, dy) + dz2 * (3.0 * wkd(nz - 1, dx, dy) - wkd(nz - 2, dx, dy));
+                return (T)((dx ? dmul(kx, ng) : dmul(ky, ng)) * sa);
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int m = o / nsp, k = o - m * nsp;
+                const size_t base = (size_t)m * L * n2 + iy + ng * ix;
+                if (k == 0) { D[base] = val; return; }
+                if (k < 4 * nz - 3) {
+                    const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
+                    T* out = kind == 0 ? A : kind == 1 ? B : kind == 2 ? C : D;
+                    out[base + (size_t)iz * n2] = val;
                     return;
                 }
-                ctl[3 * m + 1] = it + 1;
-                if (!(e > toler) || it + 1 >= nitmax) {
-                    ctl[3 * m] = 0;
-                    if (it + 1 >= nitmax) ctl[3 * m + 2] = SW_ERR_PSOLVE_MAXITER;
-                }
+                ((k == 4 * nz - 3) ? A : B)[base + (size_t)nz * n2] = val;
             });
-            sweeps++;
-            int* hctl = reinterpret_cast<int*>(h_pinned);
-            SW_CUDA(cudaMemcpyAsync(hctl, ctl, sizeof(int) * 3 * M, cudaMemcpyDeviceToHost, st));
-            SW_CUDA(cudaStreamSynchronize(st));
-            bool any = false;
-            for (int m = 0; m < M; m++) any = any || hctl[3 * m];
-            if (!any || sweeps >= nitmax) break;
+        // (b) total source S = S0 + S1(p), to spectral space
+        fft.ptospc(st, ML,
+            [=] __device__(int q, int iy, int ix) -> T {
+                const int m = q / L, iz = q % L;
+                const int i = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + i;
+                const size_t cb = (size_t)m * L * n2 + i;
+                double s;
+                if (iz == 0) {
+                    s = (double)SP0[p] + (double)C2[p] * (double)D[p];
+                } else if (iz < nz) {
+                    s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
+                    s += (double)C2[p] * (double)D[p] + (double)C1[p] * (double)C[p];
+                } else {
+                    const double d1 = D[cb + (size_t)(nz - 1) * n2], d2 = D[cb + (size_t)(nz - 2) * n2];
+                    const double dpdt = (double)C[cb + (size_t)(nz - 1) * n2] + dz2 * (3.0 * d1 - d2);
+                    const double d2pdt2 = 2.0 * d1 - d2;
+                    s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
+                    s += (double)C2[p] * d2pdt2 + (double)C1[p] * dpdt;
+                }
+                return (T)s;
+            },
+            [=] __device__(int q, int kx, int ky, T val) { SP[(size_t)q * n2 + kx + ng * ky] = val; });
+        // (c) compact RHS and Thomas solve per (kx, ky) column; residual terms
+        double* cterm = WD(1);  // per column: [num, den] packed as two planes of M*n2
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            const size_t cb = (size_t)m * L * n2 + i;
+            double* num = cterm + c;
+            double* den = cterm + (size_t)M * n2 + c;
+            if (!ctl[3 * m]) { *num = 0.0; *den = 0.0; return; }
+            // forward elimination: x(iz) stored in PS, sp(iz) streamed (no local arrays)
+            const double api = ap[i];
+            double spm = (double)SP[cb], spc = (double)SP[cb + n2];
+            double x = ((1.0 / 3.0) * spm + (1.0 / 6.0) * spc) * htdv[i];
+            PS[cb] = x;
+            for (int iz = 1; iz < nz; iz++) {
+                const double spp = (double)SP[cb + (size_t)(iz + 1) * n2];
+                const double g = (1.0 / 12.0) * (spm + spp) + (5.0 / 6.0) * spc;
+                x = (g - api * x) * htdv[i + (size_t)n2 * iz];
+                PS[cb + (size_t)iz * n2] = x;
+                spm = spc;
+                spc = spp;
+            }
+            // back substitution with the residual terms of errp
+            const int kx = i % ng, ky = i / ng;
+            const double wgt = pweight(kx, ng) * pweight(ky, ng);
+            double sn = 0.0, sd = 0.0;
+            {
+                const size_t p = cb + (size_t)nz * n2;
+                const double old = PSA[p];
+                sn += old * old;
+                sd += old * old;
+                PS[p] = 0.0;
+                PSA[p] = 0.0;
+            }
+            double xn = x;
+            {
+                const size_t p = cb + (size_t)(nz - 1) * n2;
+                const double old = PSA[p];
+                sn += (xn - old) * (xn - old);
+                sd += old * old;
+                PSA[p] = xn;
+            }
+            for (int iz = nz - 2; iz >= 0; iz--) {
+                const size_t p = cb + (size_t)iz * n2;
+                const double xi = PS[p] + etdv[i + (size_t)n2 * iz] * xn;
+                const double old = PSA[p];
+                sn += (xi - old) * (xi - old);
+                sd += old * old;
+                PS[p] = xi;
+                PSA[p] = xi;
+                xn = xi;
+            }
+            *num = wgt * sn;
+            *den = wgt * sd;
+        });
+        reduce_groups<2>(st, M, n2, 0u,
+            [=] __device__(int g, long long i) {
+                RedVals<2> rv;
+                rv.v[0] = cterm[(size_t)g * n2 + i];
+                rv.v[1] = cterm[(size_t)M * n2 + (size_t)g * n2 + i];
+                return rv;
+            }, red_partial.p, red_out.p);
+        // (d) convergence control (psolve.rs:89, 339-358)
+        const double* sums = red_out.p;
+        for_cols(st, M, [=] __device__(int m) {
+            if (!ctl[3 * m]) return;
+            const double e = sqrt(sums[2 * m] / (sums[2 * m + 1] + 1.0E-20));
+            const double eprev = ctl[3 * m + 1] > 0 ? errp[m] : 1.0;
+            const bool stagnated = mixed && e < 1.0E-4 && e > 0.7 * eprev;
+            errp[m] = e;
+            const int it = ctl[3 * m + 1];
+            if (it > 0 && e > 1.0) {
+                ctl[3 * m + 2] = SW_ERR_PSOLVE_DIVERGED;
+                ctl[3 * m] = 0;
+                ctl[3 * m + 1] = it + 1;
+                return;
+            }
+            ctl[3 * m + 1] = it + 1;
+            if (!(e > toler) || stagnated || it + 1 >= nitmax) {
+                ctl[3 * m] = 0;
+                if (it + 1 >= nitmax && !(mixed && (!(e > toler) || stagnated)))
+                    ctl[3 * m + 2] = SW_ERR_PSOLVE_MAXITER;
+            }
+        });
+        if (use_cond) {
+            long long* nexec = sweep_exec.p;
+            for_cols(st, 1, [=] __device__(int) {
+                int any = 0;
+                for (int m = 0; m < M; m++) any |= ctl[3 * m];
+                *nexec = *nexec + 1;
+                cudaGraphSetConditional(cond, any ? 1u : 0u);
+            });
         }
-        int* hctl = reinterpret_cast<int*>(h_pinned);
-        const int status0 = hctl[2];
-        int worst = SW_OK;
-        for (int m = 0; m < M; m++)
-            if (hctl[3 * m + 2] != SW_OK) worst = hctl[3 * m + 2];
-        if (iters_out) *iters_out = hctl[1];
-        if (errp_out) SW_CUDA(cudaMemcpy(errp_out, errp, sizeof(double), cudaMemcpyDeviceToHost));
-        last_psolve_iters = hctl[1];
-        if (worst != SW_OK) return worst;
+    }
+
+    // pn and dp/dtheta after convergence (psolve.rs:367-410).
+    void psolve_finish() {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+        const bool mixed = sizeof(T) == 4;
+        const double toler = mixed ? 1.0E-6 : 1.0E-9;
+        const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz2 = dz / 2.0, dz6 = dz / 6.0;
+        const double dzisq = (1.0 / dz) * (1.0 / dz);
+        const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
+        const double *filt = op.filt, *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap, *htd1 = op.htd1, *etd1 = op.etd1;
+        T *R = r, *RI = ri, *PN = pn, *DPN = dpn;
+        double* PS = ps;
+        T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
+        T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
+        double* PSA = WD(0);
+        int* ctl = ctrl.p;
+        double* errp = errp_d.p;
+        (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;
+        (void)SIGX; (void)SIGY; (void)C1; (void)C2; (void)SP0; (void)A; (void)B; (void)C; (void)D; (void)ctl; (void)errp;
+        (void)htdv; (void)etdv; (void)ap; (void)dz2; (void)dzisq; (void)hdzi; (void)mixed;
         // pn = spctop(ps), levels 0..nz-1; pn(nz) = 0
         fft.spctop(st, ML,
             [=] __device__(int q, int kx, int ky) -> T { return (T)PS[(size_t)q * n2 + kx + ng * ky]; },
@@ -686,15 +826,22 @@ struct Solver {
         for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
             const size_t cb = (size_t)m * L * n2 + i;
-            double g[MAX_NZ + 1];
             auto P = [&](int iz) { return PS[cb + (size_t)iz * n2]; };
-            for (int iz = 1; iz < nz; iz++) g[iz] = (P(iz + 1) - P(iz - 1)) * hdzi;
-            g[nz] = dz6 * (double)SP[cb + (size_t)nz * n2] - P(nz - 1) * dzi;
-            g[1] *= htd1[0];
-            for (int iz = 2; iz < nz; iz++) g[iz] = (g[iz] - (1.0 / 6.0) * g[iz - 1]) * htd1[iz - 1];
-            g[nz] = (g[nz] - (1.0 / 3.0) * g[nz - 1]) * htd1[nz - 1];
-            for (int iz = nz - 1; iz >= 1; iz--) g[iz] += etd1[iz - 1] * g[iz + 1];
-            for (int iz = 1; iz <= nz; iz++) GG[cb + (size_t)iz * n2] = g[iz];
+            auto G = [&](int iz) -> double& { return GG[cb + (size_t)iz * n2]; };
+            // forward elimination of the compact scheme, levels 1..nz (streamed through GG)
+            double gprev = (P(2) - P(0)) * hdzi * htd1[0];
+            G(1) = gprev;
+            for (int iz = 2; iz < nz; iz++) {
+                gprev = ((P(iz + 1) - P(iz - 1)) * hdzi - (1.0 / 6.0) * gprev) * htd1[iz - 1];
+                G(iz) = gprev;
+            }
+            double gn = dz6 * (double)SP[cb + (size_t)nz * n2] - P(nz - 1) * dzi;
+            gn = (gn - (1.0 / 3.0) * gprev) * htd1[nz - 1];
+            G(nz) = gn;
+            for (int iz = nz - 1; iz >= 1; iz--) {
+                gn = G(iz) + etd1[iz - 1] * gn;
+                G(iz) = gn;
+            }
         });
         const int Mnz = M * nz;
         fft.spctop(st, Mnz,
@@ -706,7 +853,75 @@ struct Solver {
                 const int m = o / nz, iz = 1 + o % nz;
                 DPN[(size_t)(m * L + iz) * n2 + iy + ng * ix] = val;
             });
+    }
+
+    // Host-driven psolve (psolve.rs:16-411): one stream sync per sweep.  Returns
+    // the worst member status; outputs are left untouched on failure, as the
+    // reference quits there.
+    int psolve(int nitmax, int* iters_out, double* errp_out) {
+        if (nitmax <= 0) nitmax = 100;
+        psolve_prepare(nitmax);
+        int sweeps = 0;
+        int* hctl = reinterpret_cast<int*>(h_pinned);
+        while (true) {
+            psolve_sweep(nitmax, false, 0);
+            sweeps++;
+            SW_CUDA(cudaMemcpyAsync(hctl, ctrl.p, sizeof(int) * 3 * M, cudaMemcpyDeviceToHost, st));
+            SW_CUDA(cudaStreamSynchronize(st));
+            bool any = false;
+            for (int m = 0; m < M; m++) any = any || hctl[3 * m];
+            if (!any || sweeps >= nitmax) break;
+        }
+        const int status0 = hctl[2];
+        int worst = SW_OK;
+        for (int m = 0; m < M; m++)
+            if (hctl[3 * m + 2] != SW_OK) worst = hctl[3 * m + 2];
+        if (iters_out) *iters_out = hctl[1];
+        if (errp_out) SW_CUDA(cudaMemcpy(errp_out, errp_d.p, sizeof(double), cudaMemcpyDeviceToHost));
+        last_psolve_iters = hctl[1];
+        if (worst != SW_OK) return worst;
+        psolve_finish();
         return status0;
+    }
+
+    // psolve inside a stream capture: the sweep loop becomes a conditional WHILE
+    // node, and the sweep counts and statuses are copied to device slots `slot`.
+    void psolve_captured(int nitmax, int slot) {
+        if (nitmax <= 0) nitmax = 100;
+        psolve_prepare(nitmax);
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        SW_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+        require(cs == cudaStreamCaptureStatusActive, SW_ERR_STATE, "psolve_captured outside a capture");
+        cudaGraphConditionalHandle cond;
+        SW_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cn;
+        SW_CUDA(cudaGraphAddNode(&cn, g, deps, nd, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        SW_CUDA(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
+        cudaStream_t outer = st;
+        st = st_body;
+        SW_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        const long long c0 = launch_counter().load();
+        psolve_sweep(nitmax, true, cond);
+        k_sweep = launch_counter().load() - c0;
+        cudaGraph_t done;
+        SW_CUDA(cudaStreamEndCapture(st, &done));
+        st = outer;
+        const int M = this->M;
+        int *ctl = ctrl.p, *sw = sweeps_dev.p, *err = err_dev.p;
+        for_cols(st, M, [=] __device__(int m) {
+            sw[3 * m + slot] = ctl[3 * m + 1];
+            if (ctl[3 * m + 2] != SW_OK) atomicCAS(err, 0, ctl[3 * m + 2]);
+        });
+        psolve_finish();
     }
     int last_psolve_iters = 0;
 
@@ -833,10 +1048,10 @@ struct Solver {
     // diagnose (src/nhswps/mod.rs:666-711): records {max(u^2+v^2), max|zeta|,
     // sum of level-weighted zeta^2} per member in the history buffer.
     // ======================================================================
-    void diagnose_record() {
+    // Reduce the three diagnose quantities per member into red_out[0 .. 3M).
+    void diagnose_reduce() {
         const int n2 = this->n2, L = this->L, nz = this->nz;
         T *U = u, *V = v, *ZE = zeta;
-        double* out = diag_hist.p + (size_t)(hist_rows % hist_cap) * M * 3;
         reduce_groups<3>(st, M, (long long)L * n2, 0x3u,
             [=] __device__(int m, long long j) {
                 const int iz = (int)(j / n2);
@@ -847,8 +1062,19 @@ struct Solver {
                 rv.v[1] = fabs(ze);
                 rv.v[2] = (iz == 0 || iz == nz) ? 0.5 * ze * ze : ze * ze;
                 return rv;
-            }, red_partial.p, out);
-        hist_rows++;
+            }, red_partial.p, red_out.p);
+    }
+    // Append this step's diagnostics to the device history ring (row counter on the device).
+    void diagnose_record() {
+        diagnose_reduce();
+        const int M3 = 3 * M, cap = hist_cap;
+        double *src = red_out.p, *hist = diag_hist.p;
+        int* cnt = hist_dev.p;
+        for_cols(st, 1, [=] __device__(int) {
+            const int row = (*cnt) % cap;
+            for (int k = 0; k < M3; k++) hist[(size_t)row * M3 + k] = src[k];
+            *cnt = *cnt + 1;
+        });
     }
     void diag_finish(const double* raw, double* out4) const {
         const double vsumi = 1.0 / (double)(ng * ng * nz);
@@ -948,7 +1174,8 @@ struct Solver {
         });
     }
 
-    int advance(bool ggen) {
+    // One step with host-driven pressure loops (one stream sync per sweep).
+    int advance_direct(bool ggen) {
         int it = 0;
         double e = 0.0;
         last_sweeps[0] = last_sweeps[1] = last_sweeps[2] = 0;
@@ -970,8 +1197,92 @@ struct Solver {
             advance_update(false);
         }
         t += 1.0 / (double)ng;
+        last_from_graph = false;
         return SW_OK;
     }
+
+    // The work of one step as captured into a CUDA graph: the three pressure
+    // solves iterate inside conditional WHILE nodes, so a step needs no host
+    // round trip.
+    void advance_captured(bool ggen) {
+        SW_CUDA(cudaMemsetAsync(sweeps_dev.p, 0, sizeof(int) * 3 * M, st));
+        if (ggen) {
+            main_invert();
+            psolve_captured(100, 0);
+        }
+        diagnose_record();
+        source(WD(4), WD(5), WD(7));
+        advance_update(true);
+        for (int k = 0; k < 2; k++) {
+            main_invert();
+            psolve_captured(100, 1 + k);
+            source(WD(4), WD(5), WD(7));
+            advance_update(false);
+        }
+    }
+
+    cudaGraphExec_t step_graph(bool ggen) {
+        cudaGraphExec_t& ex = step_exec[ggen ? 1 : 0];
+        if (!ex) {
+            SW_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            const long long c0 = launch_counter().load();
+            try {
+                advance_captured(ggen);
+                // nodes captured (nothing ran): kernels outside the sweep loops
+                const long long captured = launch_counter().load() - c0;
+                k_fixed[ggen ? 1 : 0] = captured - (ggen ? 3 : 2) * k_sweep;
+                launch_counter().fetch_sub(captured);
+            } catch (...) {
+                cudaGraph_t g;
+                cudaStreamEndCapture(st, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t g;
+            SW_CUDA(cudaStreamEndCapture(st, &g));
+            SW_CUDA(cudaGraphInstantiate(&ex, g, 0));
+            SW_CUDA(cudaGraphDestroy(g));
+        }
+        return ex;
+    }
+
+    // nsteps steps as graph launches; one synchronisation at the end, where the
+    // sticky status of the pressure solves is checked.
+    int advance_graph(int nsteps, bool ggen_first) {
+        long long fixed = 0;
+        for (int k = 0; k < nsteps; k++) {
+            const bool g = k == 0 ? ggen_first : true;
+            SW_CUDA(cudaGraphLaunch(step_graph(g), st));
+            fixed += k_fixed[g ? 1 : 0];
+            t += 1.0 / (double)ng;
+        }
+        int* h = reinterpret_cast<int*>(h_pinned);
+        long long* hx = reinterpret_cast<long long*>(h_pinned + 4);
+        SW_CUDA(cudaMemcpyAsync(h, err_dev.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaMemcpyAsync(h + 1, sweeps_dev.p, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaMemcpyAsync(hx, sweep_exec.p, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaMemsetAsync(sweep_exec.p, 0, sizeof(long long), st));
+        SW_CUDA(cudaStreamSynchronize(st));
+        count_launch(fixed + hx[0] * k_sweep);
+        for (int i = 0; i < 3; i++) last_sweeps[i] = h[1 + i];
+        last_from_graph = true;
+        if (h[0] != SW_OK) {
+            SW_CUDA(cudaMemset(err_dev.p, 0, sizeof(int)));
+            return h[0];
+        }
+        return SW_OK;
+    }
+
+    int advance(int nsteps, bool ggen_first) {
+        if (use_graphs) return advance_graph(nsteps, ggen_first);
+        for (int k = 0; k < nsteps; k++) {
+            int stt = advance_direct(k == 0 ? ggen_first : true);
+            if (stt) return stt;
+        }
+        return SW_OK;
+    }
+    bool use_graphs = true;
+    bool last_from_graph = false;
 };
 
 }  // namespace sw

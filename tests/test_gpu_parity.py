@@ -220,3 +220,76 @@ def test_advance_golden(sw, ng, nz, t0):
     for name in FIELDS:
         _close(st.get(name), expect("advance", case, name), 1e-10)
     assert abs(st.t - (t0 + 1.0 / ng)) < 1e-12
+
+
+# ---- multi-step runs against the FP64 oracle (config: ng=32, nz=4, vstrip -> balinit,
+# q + N(0, 1e-3) seed 1, delta = gamma = 0, 10 steps) ---------------------------------
+def _config0(sw, oracle, precision, steps):
+    ng, nz = 32, 4
+    qq0 = oracle.vstrip(ng)
+    qb, _, _ = oracle.balinit(ng, nz, qq0)
+    rng = np.random.default_rng(1)
+    q3 = np.tile(qb, nz + 1) + rng.normal(0.0, 1.0e-3, ng * ng * (nz + 1))
+    z3 = np.zeros_like(q3)
+    sp = sw.Spectral(ng, nz, precision=precision)
+    st = sw.nhswps.initial_state(sp, q3, z3, z3)
+    st.ggen = True
+    osp, ost = oracle.initial_state(ng, nz, q3, z3, z3)
+    for _ in range(steps):
+        sw.nhswps.advance(st)
+        status, _, _ = oracle.advance(osp, ost, ggen=True)
+        assert status == 0
+    return st, ost
+
+
+def _h(f, nz):
+    """h = z(nz)/HBAR - 1 per horizontal point."""
+    return f[-f.size // (nz + 1):] / 0.4 - 1.0
+
+
+def test_fp64_ten_steps_vs_oracle(sw, oracle):
+    st, ost = _config0(sw, oracle, sw.SW_FP64, 10)
+    for k in ("qs", "ds", "gs", "u", "v", "z", "pn"):
+        err = rel_l2(st.get(k), ost.f[k])
+        assert err <= 1e-11, "%s rel-L2 %.3e" % (k, err)
+
+
+def test_mixed_ten_steps_vs_oracle(sw, oracle):
+    st, ost = _config0(sw, oracle, sw.SW_MIXED, 10)
+    for k in ("qs", "ds", "gs", "u", "v", "z"):
+        err = rel_l2(st.get(k), ost.f[k])
+        assert err <= 1e-5, "%s rel-L2 %.3e" % (k, err)
+
+
+def test_graph_steps_match_host_driven_steps(sw):
+    """A step run as one CUDA graph (device-side pressure loops) gives the same
+    fields, bit for bit, as the host-driven path."""
+    import ctypes
+    ng, nz = 32, 4
+    qq = sw.vstrip.pv_strip(ng)
+    rng = np.random.default_rng(3)
+    q3 = np.tile(qq, nz + 1) + rng.normal(0.0, 1.0e-3, ng * ng * (nz + 1))
+    z3 = np.zeros_like(q3)
+    out = []
+    for graphs in (1, 0):
+        sp = sw.Spectral(ng, nz)
+        sw._native.check(sw._native.lib().sw_set_graphs(sp.ctx, graphs))
+        st = sw.nhswps.initial_state(sp, q3, z3, z3)
+        st.ggen = True
+        sw.nhswps.advance(st, nsteps=3)
+        out.append({k: st.get(k) for k in ("qs", "ds", "gs", "pn", "dpn", "w")})
+        out[-1]["sweeps"] = sw.nhswps.last_sweeps(sp)
+    for k in ("qs", "ds", "gs", "pn", "dpn", "w"):
+        assert np.array_equal(out[0][k], out[1][k]), k
+    assert out[0]["sweeps"] == out[1]["sweeps"]
+
+
+def test_psolve_iteration_cap_raises(sw):
+    """An unreachable sweep cap returns SW_ERR_PSOLVE_MAXITER (the reference quits,
+    src/nhswps/psolve.rs:360-366), with the GPU context still usable."""
+    st = gpu_state(sw, "psolve", "24_4", 24, 4)
+    with pytest.raises(sw.SwError) as e:
+        sw.nhswps.psolve(st, nitmax=1)
+    assert e.value.status == sw._native.SW_ERR_PSOLVE_MAXITER
+    it, errp = sw.nhswps.psolve(gpu_state(sw, "psolve", "24_4", 24, 4))
+    assert it > 1 and errp <= 1e-9
