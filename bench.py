@@ -153,6 +153,22 @@ def run_reference(args, rank, world):
     return 0
 
 
+def max_over_ranks(x, world, device="cpu"):
+    """Maximum of a per-rank float over all ranks (identity for one rank)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, t_local, world, device="cpu"):
+    """Whole-job units/s for independent replicas: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / max_over_ranks(t_local, world, device)
+
+
 def time_fft_pass(sw, sp, planes, w_fft, reps=20):
     """Average duration of one batched 2-D transform pass over `planes` planes,
     CUDA events on the library's stream; returns (seconds per launch, bytes per launch)."""
@@ -198,6 +214,8 @@ def main():
     ap.add_argument("--fft-only", action="store_true",
                     help="only time the batched 2-D transform pass (for profiling the top kernel)")
     ap.add_argument("--planes", type=int, default=6 * (NZ + 1))
+    ap.add_argument("--graphs", default="on", choices=["on", "off"],
+                    help="run each step as one CUDA graph (on) or host-driven (off; same kernels, for profiling)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -218,6 +236,7 @@ def main():
     w_fft = 8 if prec == sw.SW_FP64 else 4
 
     sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+    sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
     if args.fft_only:
         return fft_only(sw, sp, args, w_fft)
     q3, d3, g3 = initial_fields(NG, NZ, 1 + rank, sw.vstrip.pv_strip)
@@ -254,13 +273,7 @@ def main():
     sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n1)))
     ms = e0.elapsed_time(e1)
     t_local = ms / 1e3
-    if world > 1:
-        t = torch.tensor([t_local], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    else:
-        t_max = t_local
-    value = world * args.steps / t_max
+    value = replica_throughput(args.steps, t_local, world, "cuda")
     launches = int(n1.value - n0.value)
 
     # ---- end-to-end through the C ABI with host buffers ---------------------------------
@@ -282,11 +295,7 @@ def main():
             sw._native.check(L.sw_state_get(sp.ctx, fidx[k], 0, ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
     torch.cuda.synchronize()
     e2e_local = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_local], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_local = float(t.item())
-    e2e_value = world * e2e_steps / e2e_local
+    e2e_value = replica_throughput(e2e_steps, e2e_local, world, "cuda")
 
     # ---- dominant kernel: batched 2-D transform pass, timed live ---------------------
     peak, peak_kind = measured_peak()
