@@ -142,6 +142,18 @@ int sw_stream(sw_ctx* ctx, void** stream);
  * work precision (double for SW_FP64, float for SW_MIXED); in and out may alias.
  * Launches two tile passes per call (reference D2FFT::ptospc/spctop, src/sta2dfft.rs:91-123). */
 int sw_fft2d_dev(sw_ctx* ctx, int direction, int nplanes, const void* in, void* out);
+/* Allocation-free batched 2-D transforms (no counterpart in the reference).
+ * Same transforms as sw_fft2d_dev, float64, but needing no context and calling
+ * no cudaMalloc: for callers that cannot allocate device memory where they
+ * transform (a plugin inside a framework that owns the device memory pool, code
+ * being captured into someone else's CUDA graph, allocation-free real-time loops).
+ * in/out are the caller's device buffers of nplanes ng*ng planes (may alias);
+ * stream is a cudaStream_t.  Scratch is a fixed 16 MiB array inside the library,
+ * held by every GPU that loads it until exit; ng is limited to 1024 (larger sizes
+ * return SW_ERR_ARG).  All calls share that array: calls overlapping on the GPU
+ * race, so serialise them on one stream.  The first call on a device looks the
+ * array's address up; make it before any stream capture that records this call. */
+int sw_fft2d_noalloc(int ng, int direction, int nplanes, const double* in, double* out, void* stream);
 /* Number of kernels the library launched on this context so far. */
 int sw_kernel_launches(sw_ctx* ctx, long long* count);
 

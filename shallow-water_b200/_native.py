@@ -72,6 +72,7 @@ _SIGS = {
     "sw_field_device_ptr": (_i, [_vp, _i, ctypes.POINTER(_vp), _ip]),
     "sw_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
     "sw_fft2d_dev": (_i, [_vp, _i, _i, _vp, _vp]),
+    "sw_fft2d_noalloc": (_i, [_i, _i, _i, _vp, _vp, _vp]),
     "sw_kernel_launches": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
 }
 

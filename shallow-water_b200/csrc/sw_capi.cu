@@ -102,6 +102,10 @@ int fft1d_host(int m, int n, double* x, const double* trig, const int factors[5]
 
 }  // namespace
 
+namespace sw {
+void record_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace sw
+
 // ---- the context ---------------------------------------------------------------
 struct sw_ctx {
     int ng, nz, M, precision, device;
