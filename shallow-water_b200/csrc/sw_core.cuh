@@ -106,6 +106,8 @@ inline void for_planes(cudaStream_t s, int nplanes, int n2, F f) {
 }
 
 // f(c) for c < ncols: one thread per (member, horizontal point) column.
+// Column bodies loop over levels; their loops are unrolled so that loads of
+// later levels are in flight while earlier ones are used.
 template <class F>
 __global__ void k_cols(int ncols, F f) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += gridDim.x * blockDim.x) f(c);
@@ -125,6 +127,7 @@ inline void for_cols(cudaStream_t s, int ncols, F f) {
 // chunk partials of each group in fixed order.  op: 0 = sum, 1 = max.
 constexpr int RED_THREADS = 256;
 constexpr int RED_CHUNKS = 16;
+constexpr int RED_MAX_CHUNKS = 256;
 
 template <int NV>
 struct RedVals {
@@ -178,14 +181,24 @@ __global__ void k_reduce2(int ngroups, int nchunks, unsigned opmask, const doubl
 
 // Reduce ngroups groups of group_len items; f(g, i) -> RedVals<NV>; result
 // out[g*NV + v] (device).  partial must hold ngroups*RED_CHUNKS*NV doubles.
+// Chunks per group: enough CTAs for ~4 per SM overall, at least 1024 items each.
+inline int red_chunks(int ngroups, long long group_len) {
+    long long c = 592 / (ngroups > 0 ? ngroups : 1);
+    const long long by_len = group_len / 1024;
+    if (c > by_len) c = by_len;
+    if (c > RED_MAX_CHUNKS) c = RED_MAX_CHUNKS;
+    if (c < 1) c = 1;
+    return (int)c;
+}
 template <int NV, class F>
 inline void reduce_groups(cudaStream_t s, int ngroups, long long group_len, unsigned opmask, F f,
                           double* partial, double* out) {
-    dim3 g1(RED_CHUNKS, ngroups);
+    const int nch = red_chunks(ngroups, group_len);
+    dim3 g1(nch, ngroups);
     k_reduce1<NV><<<g1, RED_THREADS, 0, s>>>(group_len, opmask, f, partial);
     SW_CHECK_LAUNCH();
     const int t = ngroups * NV;
-    k_reduce2<NV><<<(t + 127) / 128, 128, 0, s>>>(ngroups, RED_CHUNKS, opmask, partial, out);
+    k_reduce2<NV><<<(t + 127) / 128, 128, 0, s>>>(ngroups, nch, opmask, partial, out);
     SW_CHECK_LAUNCH();
     count_launch(2);
 }

@@ -97,7 +97,7 @@ struct Solver {
         for (auto& b : wd) b.alloc(nf);
         plane_d.alloc((size_t)4 * M * n2);
         plane_t.alloc((size_t)4 * M * n2);
-        red_partial.alloc((size_t)RED_CHUNKS * 8 * ML + 64);
+        red_partial.alloc((size_t)RED_MAX_CHUNKS * 8 * ML + 64);
         red_out.alloc((size_t)8 * ML + 64);
         errp_d.alloc((size_t)2 * M + 2);
         diag_hist.alloc((size_t)hist_cap * M * 3);
@@ -150,6 +150,7 @@ struct Solver {
         for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
             double s = 0.0;
+            #pragma unroll 4
             for (int iz = 0; iz < L; iz++) {
                 const size_t p = (size_t)(m * L + iz) * n2 + i;
                 s += wgt[iz] * (COFI * (COFI * GS[p] - QS[p]));
@@ -193,6 +194,7 @@ struct Solver {
         for_planes(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L;
             double uio = 0.0, vio = 0.0;
+            #pragma unroll 4
             for (int iz = 0; iz < L; iz++) {
                 uio -= wgt[iz] * sums[2 * (m * L + iz)] * dsumi;
                 vio -= wgt[iz] * sums[2 * (m * L + iz) + 1] * dsumi;
@@ -225,6 +227,7 @@ struct Solver {
             double prev = dz2 * ((double)rc[0] + (double)rc[n2]);
             zc[n2] = (T)prev;
             if (mixed) zd[(size_t)m * L * n2 + i + n2] = (T)prev;
+            #pragma unroll 4
             for (int iz = 1; iz < nz; iz++) {
                 prev = prev + dz2 * ((double)rc[(size_t)iz * n2] + (double)rc[(size_t)(iz + 1) * n2]);
                 zc[(size_t)(iz + 1) * n2] = (T)prev;
@@ -288,6 +291,7 @@ struct Solver {
             const T* sc = RS + (size_t)m * L * n2 + i;
             double prev = dz2 * ((double)sc[0] + (double)sc[n2]);
             wc[n2] = (T)prev;
+            #pragma unroll 4
             for (int iz = 1; iz < nz; iz++) {
                 prev = prev + dz2 * ((double)sc[(size_t)iz * n2] + (double)sc[(size_t)(iz + 1) * n2]);
                 wc[(size_t)(iz + 1) * n2] = (T)prev;
@@ -422,12 +426,14 @@ struct Solver {
             for_cols(st, M * n2, [=] __device__(int c) {
                 const int m = c / n2, i = c - m * n2;
                 double w = 0.0;
+                #pragma unroll 4
                 for (int iz = 0; iz < L; iz++) {
                     const size_t p = (size_t)(m * L + iz) * n2 + i;
                     w += wgt[iz] * (COFI * (COFI * GS[p] - QS[p]));
                 }
                 w *= rope[i];
                 double h = 0.0, prev = 0.0;
+                #pragma unroll 4
                 for (int iz = 0; iz < L; iz++) {
                     const size_t p = (size_t)(m * L + iz) * n2 + i;
                     const double wka = COFI * (COFI * GS[p] - QS[p]) - w;
@@ -569,9 +575,13 @@ struct Solver {
     // Returns member-0 status.
     // ======================================================================
     void psolve_prepare(int nitmax) {
-        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
         require(nz >= 3, SW_ERR_ARG, "psolve needs nz >= 3");
         (void)nitmax;
+        if (fused_prepare) {
+            psolve_prepare_fused();
+            return;
+        }
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
         // Stop rule (psolve.rs:17, 89).  float64 path: the reference's 1e-9 on the
         // relative change.  float32 transforms put a floor of ~1e-6 under that
         // change, so the mixed path stops at 1e-6, or earlier once the change has
@@ -612,6 +622,347 @@ struct Solver {
                 PSA[p] = (double)val;
                 PS[p] = (iz == nz) ? 0.0 : (double)val;
             });
+        for_cols(st, M, [=] __device__(int m) {
+            ctl[3 * m] = 1;
+            ctl[3 * m + 1] = 0;
+            ctl[3 * m + 2] = SW_OK;
+        });
+    }
+
+    // psolve's set-up with vertical, coeffs and cpsource fused into eight large
+    // batched transforms (the standalone vertical()/coeffs()/cpsource() keep the
+    // reference's one-function-at-a-time order for the per-function API).  Same
+    // arithmetic except that linear steps are merged: the spectral w used for
+    // w_x, w_y is ptospc(w before the correction) + the correction's spectrum,
+    // which equals ptospc(w after it).  ux, uy, vx, vy are left in W(11..14) for
+    // source() of the same stage (u, v do not change in between).
+    void psolve_prepare_fused() {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+        const int Mnz = M * nz;
+        const bool mixed = sizeof(T) == 4;
+        const double dz2 = (HBAR / (double)nz) / 2.0;
+        const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
+        const double qdzi = (1.0 / 4.0) * (1.0 / (HBAR / (double)nz));
+        const double *filt = op.filt, *glap = op.glap, *theta = op.theta;
+        const double *DS = ds, *QS = qs, *GS = gs;
+        double *PS = ps, *PSA = WD(0);
+        T *R = r, *U = u, *V = v, *WW = w, *Z = z, *ZX = zx, *ZY = zy, *RI = ri, *AA = aa, *ZE = zeta, *PN = pn;
+        T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
+        T *Sr = W(0), *S1 = W(1), *SA = W(2), *SB = W(3), *Sx = W(17), *Sy = W(18), *Sc = W(19), *D = W(7);
+        T *RS = W(5), *Sd = W(6), *Su = W(8), *Sv = W(9), *Sw = W(10);
+        T *UX = W(11), *UY = W(12), *VX = W(13), *VY = W(14), *WX = W(15), *WY = W(16);
+        T *zd = W(20), *HZ = W(21);
+        T *Spp = W(0), *Spq = W(1), *Spr = W(2), *Pp = W(3), *Pq = W(5), *Pr = W(6), *Sq2 = W(0);
+        T* hs = plane_t.p;
+        T* hsrc = plane_t.p + (size_t)M * n2;
+        double* hspec = plane_d.p;
+        // P0: z by trapezoidal integration (+ theta); deviation kept apart for float32
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            T* zc = Z + (size_t)m * L * n2 + i;
+            const T* rc = R + (size_t)m * L * n2 + i;
+            double prev = dz2 * ((double)rc[0] + (double)rc[n2]);
+            zc[n2] = (T)prev;
+            if (mixed) zd[(size_t)m * L * n2 + i + n2] = (T)prev;
+#pragma unroll 4
+            for (int iz = 1; iz < nz; iz++) {
+                prev = prev + dz2 * ((double)rc[(size_t)iz * n2] + (double)rc[(size_t)(iz + 1) * n2]);
+                zc[(size_t)(iz + 1) * n2] = (T)prev;
+                if (mixed) zd[(size_t)m * L * n2 + i + (size_t)(iz + 1) * n2] = (T)prev;
+            }
+            for (int iz = 1; iz <= nz; iz++) zc[(size_t)iz * n2] = (T)((double)zc[(size_t)iz * n2] + theta[iz]);
+        });
+        if (mixed) {
+            // float64 spectral h deviation and vertical-mean eta (as cpsource's mixed path)
+            const double *rope = op.rope, *wgt = op.weight;
+            for_cols(st, M * n2, [=] __device__(int c) {
+                const int m = c / n2, i = c - m * n2;
+                double wv = 0.0;
+                for (int iz = 0; iz < L; iz++) {
+                    const size_t p = (size_t)(m * L + iz) * n2 + i;
+                    wv += wgt[iz] * (COFI * (COFI * GS[p] - QS[p]));
+                }
+                wv *= rope[i];
+                double h = 0.0, prev = 0.0;
+                for (int iz = 0; iz < L; iz++) {
+                    const size_t p = (size_t)(m * L + iz) * n2 + i;
+                    const double wka = COFI * (COFI * GS[p] - QS[p]) - wv;
+                    if (iz > 0) h += dz2 * (prev + wka);
+                    prev = wka;
+                }
+                hspec[c] = h;
+                hspec[(size_t)M * n2 + c] = wv;
+            });
+        }
+        const T* zsrc = mixed ? zd : Z;
+        // P1: forward transforms of everything physical that is known now
+        const int o_z = ML, o_a = ML + Mnz, o_b = o_a + ML, o_p = o_b + ML, o_u = o_p + ML, o_v = o_u + ML,
+                  o_h = o_v + ML;
+        const int n1 = o_h + (mixed ? 0 : M);
+        fft.ptospc(st, n1,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int pi = iy + ng * ix;
+                if (o < o_z) return T(1) / (R[(size_t)o * n2 + pi] + T(1));
+                if (o < o_a) {
+                    const int k = o - o_z, m = k / nz, iz = 1 + k % nz;
+                    return zsrc[(size_t)(m * L + iz) * n2 + pi];
+                }
+                if (o < o_b) { const size_t p = (size_t)(o - o_a) * n2 + pi; return U[p] * R[p]; }
+                if (o < o_p) { const size_t p = (size_t)(o - o_b) * n2 + pi; return V[p] * R[p]; }
+                if (o < o_u) return PN[(size_t)(o - o_p) * n2 + pi];
+                if (o < o_v) return U[(size_t)(o - o_u) * n2 + pi];
+                if (o < o_h) return V[(size_t)(o - o_v) * n2 + pi];
+                return Z[(size_t)((o - o_h) * L + nz) * n2 + pi];
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                if (o < o_z) { Sr[(size_t)o * n2 + i] = (T)(filt[i] * (double)val); return; }
+                if (o < o_a) {
+                    const int k = o - o_z, m = k / nz, iz = 1 + k % nz;
+                    S1[(size_t)(m * L + iz) * n2 + i] = val;
+                    return;
+                }
+                if (o < o_b) { SA[(size_t)(o - o_a) * n2 + i] = val; return; }
+                if (o < o_p) { SB[(size_t)(o - o_b) * n2 + i] = val; return; }
+                if (o < o_u) {
+                    const int q = o - o_p;
+                    const size_t p = (size_t)q * n2 + i;
+                    PSA[p] = (double)val;
+                    PS[p] = (q % L == nz) ? 0.0 : (double)val;
+                    return;
+                }
+                if (o < o_v) { Su[(size_t)(o - o_u) * n2 + i] = val; return; }
+                if (o < o_h) { Sv[(size_t)(o - o_v) * n2 + i] = val; return; }
+                hs[(size_t)(o - o_h) * n2 + i] = (T)((double)val * glap[i]);
+            });
+        // P2: inverse transforms: ri, z_x, z_y, rsrc (with A), u/v derivatives, hsrc or HZ
+        const int q_x = ML, q_r = ML + 2 * Mnz, q_d = q_r + ML, q_h = q_d + 4 * ML;
+        const int n2t = q_h + (mixed ? ML : M);
+        fft.spctop(st, n2t,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int i = kx + ng * ky;
+                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+                if (o < q_x) return Sr[(size_t)o * n2 + i];
+                if (o < q_r) {
+                    const int k = o - q_x, which = k / Mnz, kk = k - which * Mnz, m = kk / nz, iz = 1 + kk % nz;
+                    const T* sz = S1 + (size_t)(m * L + iz) * n2;
+                    return which == 0 ? (T)(dmul(kx, ng) * (double)sz[mx]) : (T)(dmul(ky, ng) * (double)sz[my]);
+                }
+                if (o < q_d) {
+                    const int q = o - q_r;
+                    const size_t b = (size_t)q * n2;
+                    const double wkb = dmul(kx, ng) * (double)SA[b + mx];
+                    const double wkc = dmul(ky, ng) * (double)SB[b + my];
+                    const T a = (T)(filt[i] * (wkb + wkc));
+                    AA[b + i] = a;
+                    return (T)((double)a + DS[b + i]);
+                }
+                if (o < q_h) {
+                    const int k = o - q_d, which = k / ML, q = k - which * ML;
+                    const T* sv = (which < 2 ? Su : Sv) + (size_t)q * n2;
+                    return (which & 1) == 0 ? (T)(dmul(kx, ng) * (double)sv[mx]) : (T)(dmul(ky, ng) * (double)sv[my]);
+                }
+                if (!mixed) return hs[(size_t)(o - q_h) * n2 + i];
+                const int q = o - q_h, m = q / L;
+                const size_t p = (size_t)q * n2 + i;
+                const double wv = hspec[(size_t)M * n2 + (size_t)m * n2 + i];
+                const double zeta_s = QS[p] + COF * (COFI * (COFI * GS[p] - QS[p]) - wv);
+                return (T)(glap[i] * hspec[(size_t)m * n2 + i] + COF * zeta_s);
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int pi = iy + ng * ix;
+                if (o < q_x) { RI[(size_t)o * n2 + pi] = val; return; }
+                if (o < q_r) {
+                    const int k = o - q_x, which = k / Mnz, kk = k - which * Mnz, m = kk / nz, iz = 1 + kk % nz;
+                    (which == 0 ? ZX : ZY)[(size_t)(m * L + iz) * n2 + pi] = val;
+                    return;
+                }
+                if (o < q_d) { RS[(size_t)(o - q_r) * n2 + pi] = -val; return; }
+                if (o < q_h) {
+                    const int k = o - q_d, which = k / ML, q = k - which * ML;
+                    T* out = which == 0 ? UX : which == 1 ? UY : which == 2 ? VX : VY;
+                    out[(size_t)q * n2 + pi] = val;
+                    return;
+                }
+                if (!mixed) hsrc[(size_t)(o - q_h) * n2 + pi] = val;
+                else HZ[(size_t)(o - q_h) * n2 + pi] = val;
+            });
+        // P3: w by trapezoidal integration of rsrc
+        for_cols(st, M * n2, [=] __device__(int c) {
+            const int m = c / n2, i = c - m * n2;
+            T* wc = WW + (size_t)m * L * n2 + i;
+            const T* sc = RS + (size_t)m * L * n2 + i;
+            double prev = dz2 * ((double)sc[0] + (double)sc[n2]);
+            wc[n2] = (T)prev;
+#pragma unroll 4
+            for (int iz = 1; iz < nz; iz++) {
+                prev = prev + dz2 * ((double)sc[(size_t)iz * n2] + (double)sc[(size_t)(iz + 1) * n2]);
+                wc[(size_t)(iz + 1) * n2] = (T)prev;
+            }
+        });
+        // P4: w, the w correction u z_x + v z_y (dealiased), ri z_x, ri z_y
+        fft.ptospc(st, 2 * Mnz + 2 * ML,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int pi = iy + ng * ix;
+                if (o < 2 * Mnz) {
+                    const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
+                    const size_t p = (size_t)(m * L + iz) * n2 + pi;
+                    return which == 0 ? WW[p] : U[p] * ZX[p] + V[p] * ZY[p];
+                }
+                const int k = o - 2 * Mnz, which = k / ML, q = k - which * ML;
+                const size_t p = (size_t)q * n2 + pi;
+                return RI[p] * (which == 0 ? ZX[p] : ZY[p]);
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                if (o < 2 * Mnz) {
+                    const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
+                    const size_t p = (size_t)(m * L + iz) * n2 + i;
+                    if (which == 0) Sw[p] = val;
+                    else Sd[p] = (T)(filt[i] * (double)val);
+                    return;
+                }
+                const int k = o - 2 * Mnz, which = k / ML, q = k - which * ML;
+                (which == 0 ? Sx : Sy)[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        // P5: w correction, w_x, w_y, sigx, sigy, div(sig)
+        fft.spctop(st, 4 * Mnz + 2 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int i = kx + ng * ky;
+                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+                if (o < 3 * Mnz) {
+                    const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
+                    const size_t b = (size_t)(m * L + iz) * n2;
+                    if (which == 0) return Sd[b + i];
+                    if (which == 1) return (T)(dmul(kx, ng) * ((double)Sw[b + mx] + (double)Sd[b + mx]));
+                    return (T)(dmul(ky, ng) * ((double)Sw[b + my] + (double)Sd[b + my]));
+                }
+                if (o < 3 * Mnz + 2 * ML) {
+                    const int k = o - 3 * Mnz, which = k / ML, q = k - which * ML;
+                    return (which == 0 ? Sx : Sy)[(size_t)q * n2 + i];
+                }
+                const int k = o - 3 * Mnz - 2 * ML, m = k / nz, iz = 1 + k % nz;
+                const size_t b = (size_t)(m * L + iz) * n2;
+                return (T)(dmul(ky, ng) * (double)Sy[b + my] + dmul(kx, ng) * (double)Sx[b + mx]);
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int pi = iy + ng * ix;
+                if (o < 3 * Mnz) {
+                    const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
+                    const size_t p = (size_t)(m * L + iz) * n2 + pi;
+                    if (which == 0) WW[p] = WW[p] + val;
+                    else (which == 1 ? WX : WY)[p] = val;
+                    return;
+                }
+                if (o < 3 * Mnz + 2 * ML) {
+                    const int k = o - 3 * Mnz, which = k / ML, q = k - which * ML;
+                    (which == 0 ? SIGX : SIGY)[(size_t)q * n2 + pi] = val;
+                    return;
+                }
+                const int k = o - 3 * Mnz - 2 * ML, m = k / nz, iz = 1 + k % nz;
+                D[(size_t)(m * L + iz) * n2 + pi] = val;
+            });
+        // P6: cpt2's argument and cpsource's dealiased products
+        fft.ptospc(st, 4 * ML,
+            [=] __device__(int o, int iy, int ix) -> T {
+                const int which = o / ML, q = o - which * ML, m = q / L, iz = q % L;
+                const int pi = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + pi;
+                if (which == 0) return T(1) - RI[p] * RI[p] - SIGX[p] * SIGX[p] - SIGY[p] * SIGY[p];
+                const size_t cb = (size_t)m * L * n2 + pi;
+                const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
+                if (which == 2 && iz == 0) return (T)((double)RI[p] * wt);
+                if (iz == 0) return T(0);
+                const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
+                const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
+                if (which == 1) return (T)(vt * (double)ZX[p] - ut * (double)ZY[p]);
+                if (which == 2) return (T)((double)UY[p] * vt - ut * (double)VY[p]);
+                return (T)(ut * (double)VX[p] - (double)UX[p] * vt);
+            },
+            [=] __device__(int o, int kx, int ky, T val) {
+                const int which = o / ML, q = o - which * ML, i = kx + ng * ky;
+                T* out = which == 0 ? Sc : which == 1 ? Spp : which == 2 ? Spq : Spr;
+                out[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        // P7: cpt2 and the products back to physical space
+        fft.spctop(st, 4 * ML,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / ML, q = o - which * ML;
+                const T* in = which == 0 ? Sc : which == 1 ? Spp : which == 2 ? Spq : Spr;
+                return in[(size_t)q * n2 + kx + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const int which = o / ML, q = o - which * ML;
+                T* out = which == 0 ? C2 : which == 1 ? Pp : which == 2 ? Pq : Pr;
+                out[(size_t)q * n2 + iy + ng * ix] = val;
+            });
+        // P8: cpt1 = 0.5 d(cpt2)/dtheta + div(sig); sig *= 2 (coeffs.rs:44-100)
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L, iz = q % L;
+            const T* c2 = C2 + (size_t)m * L * n2 + i;
+            const size_t p = (size_t)q * n2 + i;
+            double val;
+            if (iz == 0)
+                val = qdzi * (4.0 * (double)c2[n2] - 3.0 * (double)c2[0] - (double)c2[2 * (size_t)n2]);
+            else if (iz < nz)
+                val = qdzi * ((double)c2[(size_t)(iz + 1) * n2] - (double)c2[(size_t)(iz - 1) * n2]) + (double)D[p];
+            else
+                val = qdzi * (3.0 * (double)c2[(size_t)nz * n2] + (double)c2[(size_t)(nz - 2) * n2] -
+                              4.0 * (double)c2[(size_t)(nz - 1) * n2]) + (double)D[p];
+            C1[p] = (T)val;
+            SIGX[p] = SIGX[p] * T(2);
+            SIGY[p] = SIGY[p] * T(2);
+        });
+        // P9/P10: the second dealiased product and sp0 (cpsource.rs:222-258)
+        fft.ptospc(st, ML,
+            [=] __device__(int q, int iy, int ix) -> T {
+                const int m = q / L, iz = q % L;
+                if (iz == 0) return T(0);
+                const int pi = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + pi;
+                const size_t cb = (size_t)m * L * n2 + pi;
+                const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
+                const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
+                const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
+                double wkq = (double)Pq[p] * (double)ZX[p] + (double)Pr[p] * (double)ZY[p] - (double)WY[p] * vt;
+                wkq += ((double)UX[p] + (double)VY[p]) * wt - (double)WX[p] * ut;
+                return (T)wkq;
+            },
+            [=] __device__(int q, int kx, int ky, T val) {
+                const int i = kx + ng * ky;
+                Sq2[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
+            });
+        fft.spctop(st, ML,
+            [=] __device__(int q, int kx, int ky) -> T { return Sq2[(size_t)q * n2 + kx + ng * ky]; },
+            [=] __device__(int q, int iy, int ix, T val) {
+                const int m = q / L, iz = q % L;
+                const int pi = iy + ng * ix;
+                const size_t p = (size_t)q * n2 + pi;
+                const double ux = UX[p], uy = UY[p], vx = VX[p], vy = VY[p];
+                double s;
+                if (mixed) {
+                    const double hz = HZ[p];
+                    if (iz == 0) {
+                        s = hz + 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
+                    } else {
+                        const double rip = RI[p];
+                        s = hz - COF * (rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
+                        s += 2.0 * (ux * vy - uy * vx);
+                    }
+                } else {
+                    const double hsv = (double)hsrc[(size_t)m * n2 + pi];
+                    if (iz == 0) {
+                        s = hsv + COF * (double)ZE[p];
+                        s += 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
+                    } else {
+                        const double rip = RI[p];
+                        s = hsv + COF * ((double)ZE[p] - rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
+                        s += 2.0 * (ux * vy - uy * vx);
+                    }
+                }
+                SP0[p] = (T)s;
+            });
+        int* ctl = ctrl.p;
         for_cols(st, M, [=] __device__(int m) {
             ctl[3 * m] = 1;
             ctl[3 * m + 1] = 0;
@@ -715,6 +1066,7 @@ struct Solver {
             double spm = (double)SP[cb], spc = (double)SP[cb + n2];
             double x = ((1.0 / 3.0) * spm + (1.0 / 6.0) * spc) * htdv[i];
             PS[cb] = x;
+            #pragma unroll 4
             for (int iz = 1; iz < nz; iz++) {
                 const double spp = (double)SP[cb + (size_t)(iz + 1) * n2];
                 const double g = (1.0 / 12.0) * (spm + spp) + (5.0 / 6.0) * spc;
@@ -743,6 +1095,7 @@ struct Solver {
                 sd += old * old;
                 PSA[p] = xn;
             }
+            #pragma unroll 4
             for (int iz = nz - 2; iz >= 0; iz--) {
                 const size_t p = cb + (size_t)iz * n2;
                 const double xi = PS[p] + etdv[i + (size_t)n2 * iz] * xn;
@@ -815,12 +1168,6 @@ struct Solver {
         (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;
         (void)SIGX; (void)SIGY; (void)C1; (void)C2; (void)SP0; (void)A; (void)B; (void)C; (void)D; (void)ctl; (void)errp;
         (void)htdv; (void)etdv; (void)ap; (void)dz2; (void)dzisq; (void)hdzi; (void)mixed;
-        // pn = spctop(ps), levels 0..nz-1; pn(nz) = 0
-        fft.spctop(st, ML,
-            [=] __device__(int q, int kx, int ky) -> T { return (T)PS[(size_t)q * n2 + kx + ng * ky]; },
-            [=] __device__(int q, int iy, int ix, T val) {
-                PN[(size_t)q * n2 + iy + ng * ix] = (q % L == nz) ? T(0) : val;
-            });
         // dp/dtheta by 4th-order compact differences (psolve.rs:371-410), levels 1..nz
         double* GG = WD(1);
         for_cols(st, M * n2, [=] __device__(int c) {
@@ -831,6 +1178,7 @@ struct Solver {
             // forward elimination of the compact scheme, levels 1..nz (streamed through GG)
             double gprev = (P(2) - P(0)) * hdzi * htd1[0];
             G(1) = gprev;
+            #pragma unroll 4
             for (int iz = 2; iz < nz; iz++) {
                 gprev = ((P(iz + 1) - P(iz - 1)) * hdzi - (1.0 / 6.0) * gprev) * htd1[iz - 1];
                 G(iz) = gprev;
@@ -838,19 +1186,26 @@ struct Solver {
             double gn = dz6 * (double)SP[cb + (size_t)nz * n2] - P(nz - 1) * dzi;
             gn = (gn - (1.0 / 3.0) * gprev) * htd1[nz - 1];
             G(nz) = gn;
+            #pragma unroll 4
             for (int iz = nz - 1; iz >= 1; iz--) {
                 gn = G(iz) + etd1[iz - 1] * gn;
                 G(iz) = gn;
             }
         });
+        // pn = spctop(ps) for levels 0..nz-1 (pn(nz) = 0) and dpn = spctop(gg) for 1..nz, one batch
         const int Mnz = M * nz;
-        fft.spctop(st, Mnz,
+        fft.spctop(st, ML + Mnz,
             [=] __device__(int o, int kx, int ky) -> T {
-                const int m = o / nz, iz = 1 + o % nz;
+                if (o < ML) return (T)PS[(size_t)o * n2 + kx + ng * ky];
+                const int k = o - ML, m = k / nz, iz = 1 + k % nz;
                 return (T)GG[(size_t)(m * L + iz) * n2 + kx + ng * ky];
             },
             [=] __device__(int o, int iy, int ix, T val) {
-                const int m = o / nz, iz = 1 + o % nz;
+                if (o < ML) {
+                    PN[(size_t)o * n2 + iy + ng * ix] = (o % L == nz) ? T(0) : val;
+                    return;
+                }
+                const int k = o - ML, m = k / nz, iz = 1 + k % nz;
                 DPN[(size_t)(m * L + iz) * n2 + iy + ng * ix] = val;
             });
     }
@@ -931,19 +1286,20 @@ struct Solver {
     // ux, uy, vx, vy; W(15..16) spectral u, v; W(17..22) product spectra;
     // plane_t: z derivatives at iz = 0.
     // ======================================================================
-    void source(double* SQS, double* SDS, double* SGS) {
+    void source(double* SQS, double* SDS, double* SGS, bool reuse_uv = false) {
         const int ng = this->ng, n2 = this->n2, L = this->L, M = this->M, ML = this->ML;
         const double *filt = op.filt, *hlap = op.hlap, *c2g2 = op.c2g2, *wgt = op.weight;
         const double *QS = qs, *DS = ds, *PSp = ps;
         T *U = u, *V = v, *RI = ri, *DPN = dpn, *Z = z, *ZX = zx, *ZY = zy, *AA = aa;
         T *Q = W(5), *DD = W(6), *F = W(7), *FF = W(8), *FX = W(9), *FY = W(10);
         T *UX = W(11), *UY = W(12), *VX = W(13), *VY = W(14), *Su = W(15), *Sv = W(16);
-        T* S[6] = {W(17), W(18), W(19), W(20), W(21), W(22)};
-        T *S0 = S[0], *S1 = S[1], *S2 = S[2], *S3 = S[3], *S4 = S[4], *S5 = S[5];
+        T *S0 = W(17), *S1 = W(18), *S2 = W(19), *S3 = W(20), *S4 = W(21), *S5 = W(22);
         T* zs0 = plane_t.p;                       // spectral z(0)
         T* zx0 = plane_t.p + (size_t)M * n2;      // d/dx z(0)
         T* zy0 = plane_t.p + (size_t)2 * M * n2;  // d/dy z(0)
         double* wkd = plane_d.p;
+        // ux, uy, vx, vy are those psolve's set-up left in W(11..14) when reuse_uv
+        const int nuv = reuse_uv ? 0 : 2;
         // wkd = c2g2 * <A>
         for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
@@ -951,57 +1307,51 @@ struct Solver {
             for (int iz = 0; iz < L; iz++) s += wgt[iz] * (double)AA[(size_t)(m * L + iz) * n2 + i];
             wkd[c] = s * c2g2[i];
         });
-        // q and delta in physical space
-        fft.spctop(st, 2 * ML,
-            [=] __device__(int o, int kx, int ky) -> T {
-                const int which = o / ML, q = o - which * ML;
-                return (T)(which == 0 ? QS : DS)[(size_t)q * n2 + kx + ng * ky];
-            },
-            [=] __device__(int o, int iy, int ix, T val) {
-                const int which = o / ML, q = o - which * ML;
-                (which == 0 ? Q : DD)[(size_t)q * n2 + iy + ng * ix] = val;
-            });
-        // F = deal(ri * dpn) spectral; spectral u, v; spectral z(0)
-        fft.ptospc(st, 3 * ML + M,
+        // F = deal(ri * dpn) spectral; spectral u, v (unless reused); spectral z(0)
+        const int nf1 = (1 + nuv) * ML;
+        fft.ptospc(st, nf1 + M,
             [=] __device__(int o, int iy, int ix) -> T {
-                if (o >= 3 * ML) return Z[(size_t)((o - 3 * ML) * L) * n2 + iy + ng * ix];
+                if (o >= nf1) return Z[(size_t)((o - nf1) * L) * n2 + iy + ng * ix];
                 const int which = o / ML, q = o - which * ML;
                 const size_t p = (size_t)q * n2 + iy + ng * ix;
                 return which == 0 ? RI[p] * DPN[p] : which == 1 ? U[p] : V[p];
             },
             [=] __device__(int o, int kx, int ky, T val) {
                 const int i = kx + ng * ky;
-                if (o >= 3 * ML) { zs0[(size_t)(o - 3 * ML) * n2 + i] = val; return; }
+                if (o >= nf1) { zs0[(size_t)(o - nf1) * n2 + i] = val; return; }
                 const int which = o / ML, q = o - which * ML;
                 if (which == 0) F[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
                 else (which == 1 ? Su : Sv)[(size_t)q * n2 + i] = val;
             });
-        // ff, ffx, ffy, ux, uy, vx, vy, and z(0) derivatives
-        fft.spctop(st, 7 * ML + 2 * M,
+        // q, delta, ff, ffx, ffy, (ux, uy, vx, vy), z(0) derivatives to physical space
+        const int nf2 = (5 + 2 * nuv) * ML;
+        fft.spctop(st, nf2 + 2 * M,
             [=] __device__(int o, int kx, int ky) -> T {
                 const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
-                if (o >= 7 * ML) {
-                    const int which = (o - 7 * ML) / M, m = (o - 7 * ML) % M;
+                if (o >= nf2) {
+                    const int which = (o - nf2) / M, m = (o - nf2) % M;
                     const T* s = zs0 + (size_t)m * n2;
                     return which == 0 ? (T)(dmul(kx, ng) * (double)s[mx]) : (T)(dmul(ky, ng) * (double)s[my]);
                 }
                 const int which = o / ML, q = o - which * ML;
-                const T* s = (which < 3 ? F : which < 5 ? Su : Sv) + (size_t)q * n2;
-                const int kind = which < 3 ? which : (which - 3) % 2 + 1;  // 0 value, 1 d/dx, 2 d/dy
+                if (which < 2) return (T)(which == 0 ? QS : DS)[(size_t)q * n2 + kx + ng * ky];
+                const int w2 = which - 2;  // 0..2: F, F_x, F_y; 3..6: u_x, u_y, v_x, v_y
+                const T* s = (w2 < 3 ? F : w2 < 5 ? Su : Sv) + (size_t)q * n2;
+                const int kind = w2 < 3 ? w2 : (w2 - 3) % 2 + 1;  // 0 value, 1 d/dx, 2 d/dy
                 if (kind == 0) return s[kx + ng * ky];
                 if (kind == 1) return (T)(dmul(kx, ng) * (double)s[mx]);
                 return (T)(dmul(ky, ng) * (double)s[my]);
             },
             [=] __device__(int o, int iy, int ix, T val) {
                 const int i = iy + ng * ix;
-                if (o >= 7 * ML) {
-                    const int which = (o - 7 * ML) / M, m = (o - 7 * ML) % M;
+                if (o >= nf2) {
+                    const int which = (o - nf2) / M, m = (o - nf2) % M;
                     (which == 0 ? zx0 : zy0)[(size_t)m * n2 + i] = val;
                     return;
                 }
                 const int which = o / ML, q = o - which * ML;
-                T* out = which == 0 ? FF : which == 1 ? FX : which == 2 ? FY : which == 3 ? UX : which == 4 ? UY
-                       : which == 5 ? VX : VY;
+                T* out = which == 0 ? Q : which == 1 ? DD : which == 2 ? FF : which == 3 ? FX : which == 4 ? FY
+                       : which == 5 ? UX : which == 6 ? UY : which == 7 ? VX : VY;
                 out[(size_t)q * n2 + i] = val;
             });
         // products to spectral space
@@ -1044,10 +1394,6 @@ struct Solver {
         });
     }
 
-    // ======================================================================
-    // diagnose (src/nhswps/mod.rs:666-711): records {max(u^2+v^2), max|zeta|,
-    // sum of level-weighted zeta^2} per member in the history buffer.
-    // ======================================================================
     // Reduce the three diagnose quantities per member into red_out[0 .. 3M).
     void diagnose_reduce() {
         const int n2 = this->n2, L = this->L, nz = this->nz;
@@ -1136,6 +1482,7 @@ struct Solver {
             const size_t cb = (size_t)m * L * n2 + i;
             const double dis = diss[i], rd = rdis[i], fo = fope[i], cg = c2g2[i], si = simp[i];
             double wka = 0.0, wkb = 0.0;
+            #pragma unroll 4
             for (int iz = 0; iz < L; iz++) {
                 const size_t p = cb + (size_t)iz * n2;
                 if (first) {
@@ -1159,6 +1506,7 @@ struct Solver {
             wka *= fo;
             wkb *= cg;
             double wkg = 0.0;
+            #pragma unroll 4
             for (int iz = 0; iz < L; iz++) {
                 const size_t p = cb + (size_t)iz * n2;
                 DS[p] = si * (DS[p] - wka) - dsi[p];
@@ -1167,6 +1515,7 @@ struct Solver {
                 wkg += wgt[iz] * g;
             }
             wkg *= fo;
+            #pragma unroll 4
             for (int iz = 0; iz < L; iz++) {
                 const size_t p = cb + (size_t)iz * n2;
                 GS[p] = si * (GS[p] - wkg) - gsi[p];
@@ -1186,14 +1535,14 @@ struct Solver {
             if (stt) return stt;
         }
         diagnose_record();
-        source(WD(4), WD(5), WD(7));
+        source(WD(4), WD(5), WD(7), ggen && fused_prepare);
         advance_update(true);
         for (int k = 0; k < 2; k++) {
             main_invert();
             int stt = psolve(100, &it, &e);
             last_sweeps[1 + k] = it;
             if (stt) return stt;
-            source(WD(4), WD(5), WD(7));
+            source(WD(4), WD(5), WD(7), fused_prepare);
             advance_update(false);
         }
         t += 1.0 / (double)ng;
@@ -1211,12 +1560,12 @@ struct Solver {
             psolve_captured(100, 0);
         }
         diagnose_record();
-        source(WD(4), WD(5), WD(7));
+        source(WD(4), WD(5), WD(7), ggen && fused_prepare);
         advance_update(true);
         for (int k = 0; k < 2; k++) {
             main_invert();
             psolve_captured(100, 1 + k);
-            source(WD(4), WD(5), WD(7));
+            source(WD(4), WD(5), WD(7), fused_prepare);
             advance_update(false);
         }
     }
@@ -1282,6 +1631,7 @@ struct Solver {
         return SW_OK;
     }
     bool use_graphs = true;
+    bool fused_prepare = true;  // psolve set-up as eight fused batched transforms
     bool last_from_graph = false;
 };
 
