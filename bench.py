@@ -214,6 +214,7 @@ def main():
     ap.add_argument("--fft-only", action="store_true",
                     help="only time the batched 2-D transform pass (for profiling the top kernel)")
     ap.add_argument("--planes", type=int, default=6 * (NZ + 1))
+    ap.add_argument("--members", type=int, default=1, help="ensemble members per GPU (one batched context)")
     ap.add_argument("--graphs", default="on", choices=["on", "off"],
                     help="run each step as one CUDA graph (on) or host-driven (off; same kernels, for profiling)")
     args = ap.parse_args()
@@ -235,12 +236,17 @@ def main():
     prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
     w_fft = 8 if prec == sw.SW_FP64 else 4
 
-    sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+    sp = sw.Spectral(NG, NZ, precision=prec, nmembers=args.members, device=local)
     sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
     if args.fft_only:
         return fft_only(sw, sp, args, w_fft)
-    q3, d3, g3 = initial_fields(NG, NZ, 1 + rank, sw.vstrip.pv_strip)
-    st = sw.nhswps.initial_state(sp, q3, d3, g3)
+    M = args.members
+    qq2 = sw.vstrip.pv_strip(NG)
+    for m in range(M):
+        q3, d3, g3 = initial_fields(NG, NZ, 1 + rank * M + m, lambda ng: qq2)
+        st = sw.nhswps.initial_state(sp, q3, d3, g3, member=m, invert=False)
+    sw.nhswps.main_invert_all(sp)
+    st = sw.State(sp, member=0)
     stream_ptr = ctypes.c_void_p()
     sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(stream_ptr)))
     stream = torch.cuda.ExternalStream(stream_ptr.value)
@@ -273,29 +279,29 @@ def main():
     sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n1)))
     ms = e0.elapsed_time(e1)
     t_local = ms / 1e3
-    value = replica_throughput(args.steps, t_local, world, "cuda")
+    value = replica_throughput(args.steps * M, t_local, world, "cuda")
     launches = int(n1.value - n0.value)
 
     # ---- end-to-end through the C ABI with host buffers ---------------------------------
-    n3 = sp.n3
+    n3 = sp.n3 * M
+    fidx = sw._native.FIELD_INDEX
     pinned = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
     outs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs")}
     for k in pinned:
-        pinned[k].numpy()[:] = st.get(k).ravel(order="F")
-    fidx = sw._native.FIELD_INDEX
+        sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(pinned[k].data_ptr(), sw._native._dp), n3))
     e2e_steps = max(2, min(args.steps, 5))
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         for k, buf in pinned.items():
-            sw._native.check(L.sw_state_set(sp.ctx, fidx[k], 0, ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
+            sw._native.check(L.sw_state_set_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
         sw._native.check(L.sw_advance(sp.ctx, 1, 1))
         for k, buf in outs.items():
-            sw._native.check(L.sw_state_get(sp.ctx, fidx[k], 0, ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
+            sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
     torch.cuda.synchronize()
     e2e_local = time.perf_counter() - t0
-    e2e_value = replica_throughput(e2e_steps, e2e_local, world, "cuda")
+    e2e_value = replica_throughput(e2e_steps * M, e2e_local, world, "cuda")
 
     # ---- dominant kernel: batched 2-D transform pass, timed live ---------------------
     peak, peak_kind = measured_peak()
@@ -309,7 +315,7 @@ def main():
             traffic = json.load(f).get("bytes_per_launch_%s" % args.precision)
 
     step_bytes = algorithmic_bytes_per_step(NG, NZ, float(np.mean(sweeps_seen)), w_fft)
-    step_gbs = step_bytes * (args.steps / t_local) / 1e9
+    step_gbs = step_bytes * (args.steps * M / t_local) / 1e9
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------------
     cpu = None
@@ -324,7 +330,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if w_fft == 8 else "f32+f64", "data": "synthetic",
             "config": {"workload": "nhswps advance, ng=256 nz=16, vstrip + N(0,1e-3) q, delta=gamma=0",
-                       "ng": NG, "nz": NZ, "members_per_gpu": 1, "precision": args.precision,
+                       "ng": NG, "nz": NZ, "members_per_gpu": M, "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
                        "psolve_sweeps_per_step": float(np.mean(sweeps_seen))},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * n3 * 8,

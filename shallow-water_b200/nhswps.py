@@ -249,21 +249,28 @@ def _round_half_away(x):
     return int(np.floor(abs(x) + 0.5)) * (1 if x >= 0 else -1)
 
 
-def initial_state(spectral, qq, dd, gg):
+def initial_state(spectral, qq, dd, gg, member=0, invert=True):
     """The start-up of nhswps (src/nhswps/mod.rs:238-285): physical initial
     fields (ng*ng*(nz+1) each) -> filtered spectral qs, ds, gs with zero mean,
-    then main_invert."""
+    then main_invert.  For an ensemble context, load each member with
+    invert=False and call main_invert once (it acts on all members)."""
     sp = spectral
     ng, nz = sp.ng, sp.nz
-    st = State(sp)
+    st = State(sp, member=member)
     filt = flat(sp.filt)
     for name, src in (("qs", qq), ("ds", dd), ("gs", gg)):
         fs = sp.ptospc3d(flat(src), np.zeros(sp.n3), 0, nz).reshape(nz + 1, ng * ng)
         fs[:, 0] = 0.0
         fs *= filt[None, :]
         st.set(name, fs.reshape(-1))
-    check(lib().sw_main_invert(sp.ctx))
+    if invert:
+        check(lib().sw_main_invert(sp.ctx))
     return st
+
+
+def main_invert_all(spectral):
+    """main_invert for every member of the context (src/spectral/mod.rs:305-417)."""
+    check(lib().sw_main_invert(spectral.ctx))
 
 
 def _read_r8(path):

@@ -293,3 +293,58 @@ def test_psolve_iteration_cap_raises(sw):
     assert e.value.status == sw._native.SW_ERR_PSOLVE_MAXITER
     it, errp = sw.nhswps.psolve(gpu_state(sw, "psolve", "24_4", 24, 4))
     assert it > 1 and errp <= 1e-9
+
+
+def test_ensemble_members_match_single_runs(sw):
+    """Members of one batched context evolve exactly like separate single runs
+    (each member its own seed; no coupling between members)."""
+    ng, nz, M, steps = 32, 4, 3, 2
+    qq = sw.vstrip.pv_strip(ng)
+    inits = []
+    for m in range(M):
+        rng = np.random.default_rng(100 + m)
+        inits.append(np.tile(qq, nz + 1) + rng.normal(0.0, 1.0e-3, ng * ng * (nz + 1)))
+    z3 = np.zeros_like(inits[0])
+    ens = sw.Spectral(ng, nz, nmembers=M)
+    states = [sw.nhswps.initial_state(ens, q, z3, z3, member=m, invert=False) for m, q in enumerate(inits)]
+    sw.nhswps.main_invert_all(ens)
+    states[0].ggen = True
+    sw.nhswps.advance(states[0], nsteps=steps)
+    for m in range(M):
+        single = sw.Spectral(ng, nz)
+        st = sw.nhswps.initial_state(single, inits[m], z3, z3)
+        st.ggen = True
+        sw.nhswps.advance(st, nsteps=steps)
+        for k in ("qs", "ds", "gs", "pn", "u"):
+            err = rel_l2(states[m].get(k), st.get(k))
+            assert err <= 1e-12, "member %d %s rel-L2 %.3e" % (m, k, err)
+
+
+@pytest.mark.parametrize("ng,nz,dt,tsim", [(32, 4, 1.0 / 32, 1.0)])
+def test_nhswps_end_to_end(sw, tmp_path, ng, nz, dt, tsim):
+    """vstrip -> balinit -> swto3d -> nhswps through the package (reference
+    src/test.rs:29-40): monitor.asc and ecomp.asc match the reference's files to
+    their printed precision, and the f32 snapshots have the reference's size."""
+    params = sw.parameters.Parameters()
+    params.numerical.grid_resolution = ng
+    params.numerical.vertical_layers = nz
+    params.numerical.time_step = dt
+    params.numerical.duration = tsim
+    params.environment.output_directory = str(tmp_path)
+    sw.vstrip.init_pv_strip(params)
+    sw.balinit.balinit(params)
+    sw.swto3d.swto3d(params)
+    sw.nhswps.nhswps(params)
+    g = golden("complete")
+    for name, tol in (("monitor.asc", 1.01e-6), ("ecomp.asc", 1.01e-9)):
+        ref = np.array(bytes(g["%d_%d/%s" % (ng, nz, name)]).decode().split(), float)
+        got = np.array(open(tmp_path / name).read().split(), float)
+        assert got.shape == ref.shape, name
+        np.testing.assert_allclose(got, ref, rtol=0, atol=tol, err_msg=name)
+    for rel in ("3d/ql.r4", "2d/q.r4", "2d/h.r4"):
+        key = "%d_%d/%s" % (ng, nz, rel)
+        assert (tmp_path / rel).stat().st_size == g[key].size * 4, rel
+    # the q snapshot frames agree with the reference's f32 output
+    ref = g["%d_%d/2d/q.r4" % (ng, nz)]
+    got = np.fromfile(tmp_path / "2d/q.r4", dtype="<f4")
+    assert np.abs(got - ref).max() <= 2e-5 * max(1.0, np.abs(ref).max())
