@@ -142,8 +142,10 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "nhswps advance, ng=256 nz=16, vstrip + N(0,1e-3) q, delta=gamma=0",
-                   "ng": NG, "nz": NZ, "members": 1},
+        "config": {"workload": "nhswps advance, ng=256 nz=16, batched ensemble, vstrip + N(0,1e-3) q "
+                               "(seed per member), delta=gamma=0",
+                   "ng": NG, "nz": NZ, "members_per_gpu": args.members, "precision": "fp64",
+                   "note": "CPU members run one after another, so member-steps/s is the one-member rate"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": "%d advance step(s) of the FP64 C restatement of the reference "
                                    "(the Rust reference cannot be built here: no cargo), OpenMP over levels" % steps},
@@ -203,18 +205,104 @@ def fft_only(sw, sp, args, w_fft):
     return 0
 
 
+def run_arm(sw, args, precision, rank, world, local, full=True):
+    """Build an ensemble context, warm up, time `steps` advance steps on the device
+    (CUDA events on the library's stream) and, when `full`, the end-to-end C-ABI
+    loop with host buffers and the top kernel.  Returns a dict of results and the
+    member-0 prognostic fields after warmup + steps."""
+    import torch
+    L = sw._native.lib()
+    prec = sw.SW_FP64 if precision == "fp64" else sw.SW_MIXED
+    w_fft = 8 if prec == sw.SW_FP64 else 4
+    M = args.members
+    sp = sw.Spectral(NG, NZ, precision=prec, nmembers=M, device=local)
+    sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
+    qq2 = sw.vstrip.pv_strip(NG)
+    for m in range(M):
+        q3, d3, g3 = initial_fields(NG, NZ, 1 + rank * M + m, lambda ng: qq2)
+        sw.nhswps.initial_state(sp, q3, d3, g3, member=m, invert=False)
+    sw.nhswps.main_invert_all(sp)
+    st = sw.State(sp, member=0)
+    stream_ptr = ctypes.c_void_p()
+    sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        sw._native.check(L.sw_advance(sp.ctx, 1, 1))
+    sw.nhswps.diag_history(sp)
+    sweeps_seen = []
+    n0, n1 = ctypes.c_longlong(), ctypes.c_longlong()
+    barrier()
+    torch.cuda.synchronize()
+    sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n0)))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            sw._native.check(L.sw_advance(sp.ctx, 1, 1))
+            sweeps_seen.append(sum(sw.nhswps.last_sweeps(sp)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n1)))
+    ms = e0.elapsed_time(e1)
+    t_local = ms / 1e3
+    res = {
+        "precision": precision, "w_fft": w_fft, "ms": ms, "t_local": t_local,
+        "value": replica_throughput(args.steps * M, t_local, world, "cuda"),
+        "launches": int(n1.value - n0.value), "sweeps": float(np.mean(sweeps_seen)), "clocks": clk.summary(),
+        "snapshot": {k: st.get(k).ravel(order="F") for k in ("qs", "ds", "gs", "pn")},
+    }
+    if full:
+        n3 = sp.n3 * M
+        fidx = sw._native.FIELD_INDEX
+        pinned = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
+        outs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs")}
+        for k in pinned:
+            sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(pinned[k].data_ptr(), sw._native._dp), n3))
+        e2e_steps = max(2, min(args.steps, 5))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for k, buf in pinned.items():
+                sw._native.check(L.sw_state_set_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
+            sw._native.check(L.sw_advance(sp.ctx, 1, 1))
+            for k, buf in outs.items():
+                sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
+        torch.cuda.synchronize()
+        e2e_local = time.perf_counter() - t0
+        res["e2e"] = {"value": replica_throughput(e2e_steps * M, e2e_local, world, "cuda"), "unit": UNIT,
+                      "h2d_bytes_per_step": 4 * n3 * 8, "d2h_bytes_per_step": 3 * n3 * 8, "steps": e2e_steps}
+        planes = 6 * (NZ + 1)
+        per_launch_s, bytes_per_launch = time_fft_pass(sw, sp, planes, w_fft)
+        res["fft"] = {"planes": planes, "per_launch_s": per_launch_s, "bytes": bytes_per_launch}
+    sp.close()
+    torch.cuda.synchronize()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="precision of the timed (headline) path")
+    ap.add_argument("--members", type=int, default=8, help="ensemble members per GPU (one batched context)")
+    ap.add_argument("--compare", default="on", choices=["on", "off"],
+                    help="also time the other precision on the same ensemble and report the ratio and the "
+                         "mixed-vs-FP64 rel-L2 after the timed steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fft-only", action="store_true",
                     help="only time the batched 2-D transform pass (for profiling the top kernel)")
     ap.add_argument("--planes", type=int, default=6 * (NZ + 1))
-    ap.add_argument("--members", type=int, default=1, help="ensemble members per GPU (one batched context)")
     ap.add_argument("--graphs", default="on", choices=["on", "off"],
                     help="run each step as one CUDA graph (on) or host-driven (off; same kernels, for profiling)")
     args = ap.parse_args()
@@ -232,117 +320,67 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     sw = load_package()
-    L = sw._native.lib()
-    prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
-    w_fft = 8 if prec == sw.SW_FP64 else 4
-
-    sp = sw.Spectral(NG, NZ, precision=prec, nmembers=args.members, device=local)
-    sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
     if args.fft_only:
-        return fft_only(sw, sp, args, w_fft)
+        prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
+        sp = sw.Spectral(NG, NZ, precision=prec, nmembers=1, device=local)
+        return fft_only(sw, sp, args, 8 if prec == sw.SW_FP64 else 4)
+
+    main_arm = run_arm(sw, args, args.precision, rank, world, local, full=True)
+    other = None
+    if args.compare == "on":
+        other = run_arm(sw, args, "fp64" if args.precision == "mixed" else "mixed", rank, world, local, full=False)
+
     M = args.members
-    qq2 = sw.vstrip.pv_strip(NG)
-    for m in range(M):
-        q3, d3, g3 = initial_fields(NG, NZ, 1 + rank * M + m, lambda ng: qq2)
-        st = sw.nhswps.initial_state(sp, q3, d3, g3, member=m, invert=False)
-    sw.nhswps.main_invert_all(sp)
-    st = sw.State(sp, member=0)
-    stream_ptr = ctypes.c_void_p()
-    sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(stream_ptr)))
-    stream = torch.cuda.ExternalStream(stream_ptr.value)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    # ---- warm-up ---------------------------------------------------------------
-    for _ in range(args.warmup):
-        sw._native.check(L.sw_advance(sp.ctx, 1, 1))
-    sw.nhswps.diag_history(sp)
-    sweeps_seen = []
-
-    # ---- device-resident timed region ------------------------------------------------
-    n0 = ctypes.c_longlong()
-    n1 = ctypes.c_longlong()
-    barrier()
-    torch.cuda.synchronize()
-    sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n0)))
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            sw._native.check(L.sw_advance(sp.ctx, 1, 1))
-            sweeps_seen.append(sum(sw.nhswps.last_sweeps(sp)))
-        e1.record(stream)
-        torch.cuda.synchronize()
-    barrier()
-    sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n1)))
-    ms = e0.elapsed_time(e1)
-    t_local = ms / 1e3
-    value = replica_throughput(args.steps * M, t_local, world, "cuda")
-    launches = int(n1.value - n0.value)
-
-    # ---- end-to-end through the C ABI with host buffers ---------------------------------
-    n3 = sp.n3 * M
-    fidx = sw._native.FIELD_INDEX
-    pinned = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
-    outs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs")}
-    for k in pinned:
-        sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(pinned[k].data_ptr(), sw._native._dp), n3))
-    e2e_steps = max(2, min(args.steps, 5))
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        for k, buf in pinned.items():
-            sw._native.check(L.sw_state_set_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
-        sw._native.check(L.sw_advance(sp.ctx, 1, 1))
-        for k, buf in outs.items():
-            sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
-    torch.cuda.synchronize()
-    e2e_local = time.perf_counter() - t0
-    e2e_value = replica_throughput(e2e_steps * M, e2e_local, world, "cuda")
-
-    # ---- dominant kernel: batched 2-D transform pass, timed live ---------------------
+    w_fft = main_arm["w_fft"]
     peak, peak_kind = measured_peak()
-    planes = 6 * (NZ + 1)
-    per_launch_s, bytes_per_launch = time_fft_pass(sw, sp, planes, w_fft)
-    achieved = bytes_per_launch / per_launch_s / 1e9
+    achieved = main_arm["fft"]["bytes"] / main_arm["fft"]["per_launch_s"] / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "fft_pass_traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
             traffic = json.load(f).get("bytes_per_launch_%s" % args.precision)
+    step_bytes = algorithmic_bytes_per_step(NG, NZ, main_arm["sweeps"], w_fft)
+    step_gbs = step_bytes * (args.steps * M / main_arm["t_local"]) / 1e9
 
-    step_bytes = algorithmic_bytes_per_step(NG, NZ, float(np.mean(sweeps_seen)), w_fft)
-    step_gbs = step_bytes * (args.steps * M / t_local) / 1e9
-
-    # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, dt = oracle_sample(1)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "1 advance step at ng=256 nz=16 of the FP64 C restatement (OpenMP over levels); %.1f s" % dt}
+               "sample": "1 advance step at ng=256 nz=16 (one member) of the FP64 C restatement "
+                         "(OpenMP over levels); %.1f s" % dt}
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if w_fft == 8 else "f32+f64", "data": "synthetic",
-            "config": {"workload": "nhswps advance, ng=256 nz=16, vstrip + N(0,1e-3) q, delta=gamma=0",
+            "metric": METRIC, "value": main_arm["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main_arm["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w_fft == 8 else "f32+f64", "data": "synthetic",
+            "config": {"workload": "nhswps advance, ng=256 nz=16, batched ensemble, vstrip + N(0,1e-3) q "
+                                   "(seed per member), delta=gamma=0",
                        "ng": NG, "nz": NZ, "members_per_gpu": M, "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
-                       "psolve_sweeps_per_step": float(np.mean(sweeps_seen))},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * n3 * 8,
-                    "d2h_bytes_per_step": 3 * n3 * 8, "steps": e2e_steps},
-            "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "k_fft_pass (batched 2-D transform pass, %d planes)" % planes,
+                       "psolve_sweeps_per_step": main_arm["sweeps"]},
+            "e2e": main_arm["e2e"],
+            "gpu_launches": main_arm["launches"],
+            "roofline": {"bound": "hbm", "kernel": "k_fft_pass (batched 2-D transform pass, %d planes)"
+                                                   % main_arm["fft"]["planes"],
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "step_algorithmic_gbs": step_gbs, "step_frac": step_gbs / peak},
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": main_arm["clocks"],
         }
+        if other is not None:
+            mixed, fp64 = (main_arm, other) if args.precision == "mixed" else (other, main_arm)
+            line["compare"] = {
+                "fp64_value": fp64["value"], "mixed_value": mixed["value"],
+                "mixed_over_fp64": mixed["value"] / fp64["value"],
+                "fp64_sweeps_per_step": fp64["sweeps"], "mixed_sweeps_per_step": mixed["sweeps"],
+                "after_steps": args.warmup + args.steps,
+                "mixed_rel_l2_vs_fp64": {k: float(np.linalg.norm(mixed["snapshot"][k] - fp64["snapshot"][k]) /
+                                                  max(np.linalg.norm(fp64["snapshot"][k]), 1e-300))
+                                         for k in ("qs", "ds", "gs", "pn")},
+                "fp64_clocks": fp64["clocks"] if args.precision == "mixed" else main_arm["clocks"],
+            }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -208,6 +208,57 @@ __device__ __forceinline__ void stockham_stage(const T2* __restrict__ x, T2* __r
     }
 }
 
+// Stockham pass with compile-time length, radix and stride (all index math
+// reduces to shifts and masks for power-of-two lengths).
+template <int R, int N, int NS, bool INV, typename T2>
+__device__ __forceinline__ void stockham_stage_s(const T2* __restrict__ x, T2* __restrict__ y,
+                                                 const T2* __restrict__ tw, int np, int pl) {
+    constexpr int nR = N / R;
+    constexpr int tstride = N / (NS * R);
+    for (int b = threadIdx.x; b < np * nR; b += FFT_THREADS) {
+        const int p = b / nR;
+        const int j = b % nR;
+        const int k = j % NS;
+        const int base = (j / NS) * NS * R + k;
+        const T2* xp = x + p * pl;
+        T2* yp = y + p * pl;
+        T2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = xp[pad16(j + r * nR)];
+        if constexpr (NS > 1) {
+            const int step = k * tstride;
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                T2 w = tw[r * step];
+                if (INV) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        butterfly<R, INV>(v);
+#pragma unroll
+        for (int r = 0; r < R; r++) yp[pad16(base + r * NS)] = v[r];
+    }
+}
+
+// Compile-time plans of the specialised lengths: 256 = 16 x 16, 128 = 16 x 8.
+template <int N, bool INV, typename T2>
+__device__ __forceinline__ T2* smem_fft_static(T2* a, T2* b, const T2* tw, int np, int pl) {
+    if constexpr (N == 256) {
+        stockham_stage_s<16, 256, 1, INV>(a, b, tw, np, pl);
+        __syncthreads();
+        stockham_stage_s<16, 256, 16, INV>(b, a, tw, np, pl);
+        __syncthreads();
+        return a;
+    } else {
+        static_assert(N == 128, "specialised lengths: 128, 256");
+        stockham_stage_s<16, 128, 1, INV>(a, b, tw, np, pl);
+        __syncthreads();
+        stockham_stage_s<8, 128, 16, INV>(b, a, tw, np, pl);
+        __syncthreads();
+        return a;
+    }
+}
+
 // Full transform of np sequences; returns the buffer holding the result.
 template <bool INV, typename T2>
 __device__ T2* smem_fft(const FftPlan& plan, T2* a, T2* b, const T2* tw, int np, int pl) {
@@ -241,12 +292,17 @@ inline size_t fft_pass_smem(int n, int tc) {
 // flight before the tile is written to shared memory.
 constexpr int FFT_UNROLL = 8;
 
-template <typename T, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
+// NS, LTCS: 0 for the general kernel (length and tile from the plan and ltc),
+// otherwise a compile-time length (128 or 256) and log2 of its tile width, so
+// that loop bounds and index arithmetic fold to constants.
+template <typename T, int NS, int LTCS, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
 __global__ void __launch_bounds__(FFT_THREADS, 3)
-k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, int ltc, FastDiv dn, T sc, LD ld, ST st) {
+k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, int ltc_rt, FastDiv dn, T sc, LD ld,
+           ST st) {
     using T2 = typename C2<T>::t;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int n = plan.n;
+    const int n = NS ? NS : plan.n;
+    const int ltc = NS ? LTCS : ltc_rt;
     const int tc = 1 << ltc;
     const int np = tc >> 1;
     const int pl = padded_len(n);
@@ -255,7 +311,7 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
     T2* buf1 = buf0 + (size_t)np * pl;
     const int o = blockIdx.y;
     const int c0 = blockIdx.x * tc;
-    const int nthr = blockDim.x;
+    const int nthr = NS ? FFT_THREADS : (int)blockDim.x;
     const int total = tc * n;
 
     for (int i = threadIdx.x; i < n; i += nthr) tw[i] = twg[i];
@@ -267,6 +323,7 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
             const int idx = base + u * nthr + threadIdx.x;
             int c, j;
             if (LOAD_CF) { c = idx & (tc - 1); j = idx >> ltc; }
+            else if (NS) { j = idx % n; c = idx / n; }
             else         { j = (int)((uint32_t)idx - fdiv((uint32_t)idx, dn) * (uint32_t)n); c = (int)fdiv((uint32_t)idx, dn); }
             const int col = c0 + c;
             vals[u] = (idx < total && col < ncols) ? (T)ld(o, col, j) : T(0);
@@ -277,6 +334,7 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
             if (idx < total) {
                 int c, j;
                 if (LOAD_CF) { c = idx & (tc - 1); j = idx >> ltc; }
+                else if (NS) { c = idx / n; j = idx % n; }
                 else         { c = (int)fdiv((uint32_t)idx, dn); j = idx - c * n; }
                 rb[(((c >> 1) * pl + pad16(j)) << 1) + (c & 1)] = vals[u];
             }
@@ -299,10 +357,14 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
         }
         __syncthreads();
     }
-    const T2* Z = smem_fft<INV>(plan, buf0, buf1, tw, np, pl);
+    const T2* Z;
+    if constexpr (NS != 0) Z = smem_fft_static<NS, INV>(buf0, buf1, tw, np, pl);
+    else Z = smem_fft<INV>(plan, buf0, buf1, tw, np, pl);
+#pragma unroll 4
     for (int idx = threadIdx.x; idx < total; idx += nthr) {
         int c, k;
         if (STORE_CF) { c = idx & (tc - 1); k = idx >> ltc; }
+        else if (NS)  { c = idx / n; k = idx % n; }
         else          { c = (int)fdiv((uint32_t)idx, dn); k = idx - c * n; }
         const int col = c0 + c;
         if (col >= ncols) continue;

@@ -111,15 +111,20 @@ template <typename T, bool INV, bool LCF, bool SCF, class LD, class ST>
 inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T>::t* tw, int tc, T sc,
                         int nout, int ncols, LD ld, ST st) {
     if (nout <= 0) return;
-    auto kern = k_fft_pass<T, INV, LCF, SCF, LD, ST>;
+    // compile-time kernels for the common lengths when the tile matches
+    constexpr int LT256 = sizeof(T) == 8 ? 4 : 5, LT128 = 5;
+    auto kern = k_fft_pass<T, 0, 0, INV, LCF, SCF, LD, ST>;
+    if (plan.n == 256 && tc == (1 << LT256)) kern = k_fft_pass<T, 256, LT256, INV, LCF, SCF, LD, ST>;
+    else if (plan.n == 128 && tc == (1 << LT128)) kern = k_fft_pass<T, 128, LT128, INV, LCF, SCF, LD, ST>;
     const size_t smem = fft_pass_smem<T>(plan.n, tc);
-    static int attr_done[64] = {0};
+    static int attr_done[64][3] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && !attr_done[dev]) {
+    const int kv = plan.n == 256 ? 1 : plan.n == 128 ? 2 : 0;
+    if (dev < 64 && !attr_done[dev][kv]) {
         SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        attr_done[dev] = 1;
+        attr_done[dev][kv] = 1;
     }
     dim3 grid((ncols + tc - 1) / tc, nout);
     kern<<<grid, FFT_THREADS, smem, s>>>(plan, tw, ncols, ilog2(tc), make_fastdiv((uint32_t)plan.n), sc, ld, st);

@@ -28,6 +28,128 @@ inline void upload(DevBuf<double>& d, const std::vector<double>& h) {
     SW_CUDA(cudaMemcpy(d.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
 }
 
+constexpr int THOMAS_THREADS = 128;
+
+// Compact fourth-order RHS and Thomas solve of one sweep (psolve.rs:285-327) for
+// one (kx, ky) column per thread; member = blockIdx.y.  Writes ps and the new
+// previous-iterate psa, and reduces the Parseval-weighted sums of
+// (ps - psa_old)^2 and psa_old^2 per CTA into part[(m*gridDim.x + blk)*2 + {0,1}].
+template <typename T>
+__global__ void __launch_bounds__(THOMAS_THREADS)
+k_thomas(int ng, int nz, int n2, const int* __restrict__ ctl, const T* __restrict__ SP,
+         const double* __restrict__ htdv, const double* __restrict__ etdv, const double* __restrict__ ap,
+         double* __restrict__ PS, double* __restrict__ PSA, double* __restrict__ part) {
+    const int m = blockIdx.y;
+    const int i = blockIdx.x * THOMAS_THREADS + threadIdx.x;
+    const int L = nz + 1;
+    double sn = 0.0, sd = 0.0;
+    if (i < n2 && ctl[3 * m]) {
+        const size_t cb = (size_t)m * L * n2 + i;
+        const double api = ap[i];
+        double spm = (double)SP[cb], spc = (double)SP[cb + n2];
+        double x = ((1.0 / 3.0) * spm + (1.0 / 6.0) * spc) * htdv[i];
+        PS[cb] = x;
+#pragma unroll 4
+        for (int iz = 1; iz < nz; iz++) {
+            const double spp = (double)SP[cb + (size_t)(iz + 1) * n2];
+            const double g = (1.0 / 12.0) * (spm + spp) + (5.0 / 6.0) * spc;
+            x = (g - api * x) * htdv[i + (size_t)n2 * iz];
+            PS[cb + (size_t)iz * n2] = x;
+            spm = spc;
+            spc = spp;
+        }
+        {
+            const size_t p = cb + (size_t)nz * n2;
+            const double old = PSA[p];
+            sn += old * old;
+            sd += old * old;
+            PS[p] = 0.0;
+            PSA[p] = 0.0;
+        }
+        double xn = x;
+        {
+            const size_t p = cb + (size_t)(nz - 1) * n2;
+            const double old = PSA[p];
+            sn += (xn - old) * (xn - old);
+            sd += old * old;
+            PSA[p] = xn;
+        }
+#pragma unroll 4
+        for (int iz = nz - 2; iz >= 0; iz--) {
+            const size_t p = cb + (size_t)iz * n2;
+            const double xi = PS[p] + etdv[i + (size_t)n2 * iz] * xn;
+            const double old = PSA[p];
+            sn += (xi - old) * (xi - old);
+            sd += old * old;
+            PS[p] = xi;
+            PSA[p] = xi;
+            xn = xi;
+        }
+        const int kx = i % ng, ky = i / ng;
+        const double wgt = pweight(kx, ng) * pweight(ky, ng);
+        sn *= wgt;
+        sd *= wgt;
+    }
+    __shared__ double sh[2][THOMAS_THREADS];
+    sh[0][threadIdx.x] = sn;
+    sh[1][threadIdx.x] = sd;
+    __syncthreads();
+    for (int w = THOMAS_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[((size_t)m * gridDim.x + blockIdx.x) * 2] = sh[0][0];
+        part[((size_t)m * gridDim.x + blockIdx.x) * 2 + 1] = sh[1][0];
+    }
+}
+
+// Convergence control of one sweep (psolve.rs:89, 339-358): per member, the
+// relative change errp from the CTA partials (fixed order), the divergence and
+// iteration-cap statuses, and the mixed path's stop rule; then, inside a graph,
+// the WHILE node's condition (any member still iterating).
+__global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, int* ctl, double* errp, double toler,
+                              int mixed, int nitmax, int use_cond, cudaGraphConditionalHandle cond,
+                              long long* nexec) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        if (!ctl[3 * m]) continue;
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < nblk; k++) {
+            a += part[((size_t)m * nblk + k) * 2];
+            b += part[((size_t)m * nblk + k) * 2 + 1];
+        }
+        const double e = sqrt(a / (b + 1.0E-20));
+        const double eprev = ctl[3 * m + 1] > 0 ? errp[m] : 1.0;
+        const bool stagnated = mixed && e < 1.0E-4 && e > 0.7 * eprev;
+        errp[m] = e;
+        const int it = ctl[3 * m + 1];
+        if (it > 0 && e > 1.0) {
+            ctl[3 * m + 2] = SW_ERR_PSOLVE_DIVERGED;
+            ctl[3 * m] = 0;
+            ctl[3 * m + 1] = it + 1;
+            continue;
+        }
+        ctl[3 * m + 1] = it + 1;
+        if (!(e > toler) || stagnated || it + 1 >= nitmax) {
+            ctl[3 * m] = 0;
+            if (it + 1 >= nitmax && !(mixed && (!(e > toler) || stagnated))) ctl[3 * m + 2] = SW_ERR_PSOLVE_MAXITER;
+        } else {
+            atomicOr(&any, 1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && use_cond) {
+        *nexec = *nexec + 1;
+        cudaGraphSetConditional(cond, any ? 1u : 0u);
+    }
+}
+
 template <typename T>
 struct Solver {
     int ng, nz, L, M, n2, ML;
@@ -1053,100 +1175,18 @@ struct Solver {
                 return (T)s;
             },
             [=] __device__(int q, int kx, int ky, T val) { SP[(size_t)q * n2 + kx + ng * ky] = val; });
-        // (c) compact RHS and Thomas solve per (kx, ky) column; residual terms
-        double* cterm = WD(1);  // per column: [num, den] packed as two planes of M*n2
-        for_cols(st, M * n2, [=] __device__(int c) {
-            const int m = c / n2, i = c - m * n2;
-            const size_t cb = (size_t)m * L * n2 + i;
-            double* num = cterm + c;
-            double* den = cterm + (size_t)M * n2 + c;
-            if (!ctl[3 * m]) { *num = 0.0; *den = 0.0; return; }
-            // forward elimination: x(iz) stored in PS, sp(iz) streamed (no local arrays)
-            const double api = ap[i];
-            double spm = (double)SP[cb], spc = (double)SP[cb + n2];
-            double x = ((1.0 / 3.0) * spm + (1.0 / 6.0) * spc) * htdv[i];
-            PS[cb] = x;
-            #pragma unroll 4
-            for (int iz = 1; iz < nz; iz++) {
-                const double spp = (double)SP[cb + (size_t)(iz + 1) * n2];
-                const double g = (1.0 / 12.0) * (spm + spp) + (5.0 / 6.0) * spc;
-                x = (g - api * x) * htdv[i + (size_t)n2 * iz];
-                PS[cb + (size_t)iz * n2] = x;
-                spm = spc;
-                spc = spp;
-            }
-            // back substitution with the residual terms of errp
-            const int kx = i % ng, ky = i / ng;
-            const double wgt = pweight(kx, ng) * pweight(ky, ng);
-            double sn = 0.0, sd = 0.0;
-            {
-                const size_t p = cb + (size_t)nz * n2;
-                const double old = PSA[p];
-                sn += old * old;
-                sd += old * old;
-                PS[p] = 0.0;
-                PSA[p] = 0.0;
-            }
-            double xn = x;
-            {
-                const size_t p = cb + (size_t)(nz - 1) * n2;
-                const double old = PSA[p];
-                sn += (xn - old) * (xn - old);
-                sd += old * old;
-                PSA[p] = xn;
-            }
-            #pragma unroll 4
-            for (int iz = nz - 2; iz >= 0; iz--) {
-                const size_t p = cb + (size_t)iz * n2;
-                const double xi = PS[p] + etdv[i + (size_t)n2 * iz] * xn;
-                const double old = PSA[p];
-                sn += (xi - old) * (xi - old);
-                sd += old * old;
-                PS[p] = xi;
-                PSA[p] = xi;
-                xn = xi;
-            }
-            *num = wgt * sn;
-            *den = wgt * sd;
-        });
-        reduce_groups<2>(st, M, n2, 0u,
-            [=] __device__(int g, long long i) {
-                RedVals<2> rv;
-                rv.v[0] = cterm[(size_t)g * n2 + i];
-                rv.v[1] = cterm[(size_t)M * n2 + (size_t)g * n2 + i];
-                return rv;
-            }, red_partial.p, red_out.p);
-        // (d) convergence control (psolve.rs:89, 339-358)
-        const double* sums = red_out.p;
-        for_cols(st, M, [=] __device__(int m) {
-            if (!ctl[3 * m]) return;
-            const double e = sqrt(sums[2 * m] / (sums[2 * m + 1] + 1.0E-20));
-            const double eprev = ctl[3 * m + 1] > 0 ? errp[m] : 1.0;
-            const bool stagnated = mixed && e < 1.0E-4 && e > 0.7 * eprev;
-            errp[m] = e;
-            const int it = ctl[3 * m + 1];
-            if (it > 0 && e > 1.0) {
-                ctl[3 * m + 2] = SW_ERR_PSOLVE_DIVERGED;
-                ctl[3 * m] = 0;
-                ctl[3 * m + 1] = it + 1;
-                return;
-            }
-            ctl[3 * m + 1] = it + 1;
-            if (!(e > toler) || stagnated || it + 1 >= nitmax) {
-                ctl[3 * m] = 0;
-                if (it + 1 >= nitmax && !(mixed && (!(e > toler) || stagnated)))
-                    ctl[3 * m + 2] = SW_ERR_PSOLVE_MAXITER;
-            }
-        });
-        if (use_cond) {
-            long long* nexec = sweep_exec.p;
-            for_cols(st, 1, [=] __device__(int) {
-                int any = 0;
-                for (int m = 0; m < M; m++) any |= ctl[3 * m];
-                *nexec = *nexec + 1;
-                cudaGraphSetConditional(cond, any ? 1u : 0u);
-            });
-        }
+        // (c) compact RHS and Thomas solve per (kx, ky) column, with the errp sums
+        //     reduced per CTA; (d) one control kernel finishes the sums per member and
+        //     applies the stop rule (psolve.rs:89, 285-358)
+        const int nblk = (n2 + THOMAS_THREADS - 1) / THOMAS_THREADS;
+        double* part = red_partial.p;
+        k_thomas<T><<<dim3(nblk, M), THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part);
+        SW_CHECK_LAUNCH();
+        count_launch();
+        k_psolve_ctrl<<<1, 256, 0, st>>>(M, nblk, part, ctl, errp, toler, mixed ? 1 : 0, nitmax, use_cond ? 1 : 0,
+                                         cond, sweep_exec.p);
+        SW_CHECK_LAUNCH();
+        count_launch();
     }
 
     // pn and dp/dtheta after convergence (psolve.rs:367-410).
