@@ -34,16 +34,54 @@ constexpr int THOMAS_THREADS = 128;
 // one (kx, ky) column per thread; member = blockIdx.y.  Writes ps and the new
 // previous-iterate psa, and reduces the Parseval-weighted sums of
 // (ps - psa_old)^2 and psa_old^2 per CTA into part[(m*gridDim.x + blk)*2 + {0,1}].
-template <typename T>
+// NZS > 0: compile-time nz; the column is kept in registers between the forward
+// elimination and the back substitution (ps is written once).
+template <typename T, int NZS>
 __global__ void __launch_bounds__(THOMAS_THREADS)
-k_thomas(int ng, int nz, int n2, const int* __restrict__ ctl, const T* __restrict__ SP,
+k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __restrict__ SP,
          const double* __restrict__ htdv, const double* __restrict__ etdv, const double* __restrict__ ap,
          double* __restrict__ PS, double* __restrict__ PSA, double* __restrict__ part) {
     const int m = blockIdx.y;
     const int i = blockIdx.x * THOMAS_THREADS + threadIdx.x;
+    const int nz = NZS ? NZS : nz_rt;
     const int L = nz + 1;
     double sn = 0.0, sd = 0.0;
-    if (i < n2 && ctl[3 * m]) {
+    if (NZS && i < n2 && ctl[3 * m]) {
+        const size_t cb = (size_t)m * L * n2 + i;
+        const double api = ap[i];
+        double sp[NZS ? NZS + 1 : 1], x[NZS ? NZS : 1];
+#pragma unroll
+        for (int iz = 0; iz <= NZS; iz++) sp[iz] = (double)SP[cb + (size_t)iz * n2];
+        x[0] = ((1.0 / 3.0) * sp[0] + (1.0 / 6.0) * sp[1]) * htdv[i];
+#pragma unroll
+        for (int iz = 1; iz < NZS; iz++) {
+            const double g = (1.0 / 12.0) * (sp[iz - 1] + sp[iz + 1]) + (5.0 / 6.0) * sp[iz];
+            x[iz] = (g - api * x[iz - 1]) * htdv[i + (size_t)n2 * iz];
+        }
+#pragma unroll
+        for (int iz = NZS - 2; iz >= 0; iz--) x[iz] += etdv[i + (size_t)n2 * iz] * x[iz + 1];
+#pragma unroll
+        for (int iz = 0; iz < NZS; iz++) {
+            const size_t p = cb + (size_t)iz * n2;
+            const double old = PSA[p];
+            sn += (x[iz] - old) * (x[iz] - old);
+            sd += old * old;
+            PS[p] = x[iz];
+            PSA[p] = x[iz];
+        }
+        {
+            const size_t p = cb + (size_t)NZS * n2;
+            const double old = PSA[p];
+            sn += old * old;
+            sd += old * old;
+            PS[p] = 0.0;
+            PSA[p] = 0.0;
+        }
+        const int kx = i % ng, ky = i / ng;
+        const double wgt = pweight(kx, ng) * pweight(ky, ng);
+        sn *= wgt;
+        sd *= wgt;
+    } else if (!NZS && i < n2 && ctl[3 * m]) {
         const size_t cb = (size_t)m * L * n2 + i;
         const double api = ap[i];
         double spm = (double)SP[cb], spc = (double)SP[cb + n2];
@@ -107,23 +145,14 @@ k_thomas(int ng, int nz, int n2, const int* __restrict__ ctl, const T* __restric
     }
 }
 
-// Convergence control of one sweep (psolve.rs:89, 339-358): per member, the
-// relative change errp from the CTA partials (fixed order), the divergence and
-// iteration-cap statuses, and the mixed path's stop rule; then, inside a graph,
-// the WHILE node's condition (any member still iterating).
-__global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, int* ctl, double* errp, double toler,
-                              int mixed, int nitmax, int use_cond, cudaGraphConditionalHandle cond,
-                              long long* nexec) {
-    __shared__ int any;
-    if (threadIdx.x == 0) any = 0;
-    __syncthreads();
-    for (int m = threadIdx.x; m < M; m += blockDim.x) {
-        if (!ctl[3 * m]) continue;
-        double a = 0.0, b = 0.0;
-        for (int k = 0; k < nblk; k++) {
-            a += part[((size_t)m * nblk + k) * 2];
-            b += part[((size_t)m * nblk + k) * 2 + 1];
-        }
+constexpr int CTRL_THREADS = 256;
+constexpr int CTRL_MAX_MEMBERS = 256;
+
+// Stop rule of one member (psolve.rs:89, 339-366).
+__device__ __forceinline__ void ctrl_member(int m, double a, double b, int* ctl, double* errp, double toler,
+                                                 int mixed, int nitmax, int* any) {
+    {
+        if (!ctl[3 * m]) return;
         const double e = sqrt(a / (b + 1.0E-20));
         const double eprev = ctl[3 * m + 1] > 0 ? errp[m] : 1.0;
         const bool stagnated = mixed && e < 1.0E-4 && e > 0.7 * eprev;
@@ -133,17 +162,59 @@ __global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, 
             ctl[3 * m + 2] = SW_ERR_PSOLVE_DIVERGED;
             ctl[3 * m] = 0;
             ctl[3 * m + 1] = it + 1;
-            continue;
+            return;
         }
         ctl[3 * m + 1] = it + 1;
         if (!(e > toler) || stagnated || it + 1 >= nitmax) {
             ctl[3 * m] = 0;
             if (it + 1 >= nitmax && !(mixed && (!(e > toler) || stagnated))) ctl[3 * m + 2] = SW_ERR_PSOLVE_MAXITER;
         } else {
-            atomicOr(&any, 1);
+            atomicOr(any, 1);
         }
     }
-    __syncthreads();
+}
+
+// Convergence control of one sweep (psolve.rs:89, 339-358): per member, the
+// relative change errp from the CTA partials (fixed order), the divergence and
+// iteration-cap statuses, and the mixed path's stop rule; then, inside a graph,
+// the WHILE node's condition (any member still iterating).
+__global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, int* ctl, double* errp, double toler,
+                              int mixed, int nitmax, int use_cond, cudaGraphConditionalHandle cond,
+                              long long* nexec) {
+    __shared__ int any;
+    __shared__ double sh[2][CTRL_THREADS];
+    __shared__ double sums[2 * CTRL_MAX_MEMBERS];
+    if (threadIdx.x == 0) any = 0;
+    // per member: strided partial sums, then a fixed-order tree (deterministic)
+    for (int m0 = 0; m0 < M; m0 += CTRL_MAX_MEMBERS) {
+        const int mcount = (M - m0 < CTRL_MAX_MEMBERS) ? M - m0 : CTRL_MAX_MEMBERS;
+        for (int mm = 0; mm < mcount; mm++) {
+            const int m = m0 + mm;
+            double a = 0.0, b = 0.0;
+            for (int k = threadIdx.x; k < nblk; k += CTRL_THREADS) {
+                a += part[((size_t)m * nblk + k) * 2];
+                b += part[((size_t)m * nblk + k) * 2 + 1];
+            }
+            sh[0][threadIdx.x] = a;
+            sh[1][threadIdx.x] = b;
+            __syncthreads();
+            for (int w = CTRL_THREADS / 2; w > 0; w >>= 1) {
+                if (threadIdx.x < w) {
+                    sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+                    sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                sums[2 * mm] = sh[0][0];
+                sums[2 * mm + 1] = sh[1][0];
+            }
+            __syncthreads();
+        }
+        for (int mm = threadIdx.x; mm < mcount; mm += CTRL_THREADS) ctrl_member(m0 + mm, sums[2 * mm], sums[2 * mm + 1],
+                                                                                 ctl, errp, toler, mixed, nitmax, &any);
+        __syncthreads();
+    }
     if (threadIdx.x == 0 && use_cond) {
         *nexec = *nexec + 1;
         cudaGraphSetConditional(cond, any ? 1u : 0u);
@@ -1113,44 +1184,22 @@ struct Solver {
         (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;
         (void)SIGX; (void)SIGY; (void)C1; (void)C2; (void)SP0; (void)A; (void)B; (void)C; (void)D; (void)ctl; (void)errp;
         (void)htdv; (void)etdv; (void)ap; (void)dz2; (void)dzisq; (void)hdzi; (void)mixed;
-        const int nsp = 4 * nz - 1;  // spctop outputs per member per sweep
-            // (a) pressure derivative terms to physical space
-        fft.spctop(st, M * nsp,
+        // (a) p, dp/dx, dp/dy to physical space for levels 0..nz-1 (p(nz) = 0).  The
+        //     theta derivatives of the reference (psolve.rs:96-240) are linear in p,
+        //     so they are formed from these in physical space in (b): 3 nz transforms
+        //     per member instead of the 4 nz - 1 of the derived quantities.
+        const int n3z = 3 * nz;
+        fft.spctop(st, M * n3z,
             [=] __device__(int o, int kx, int ky) -> T {
-                const int m = o / nsp, k = o - m * nsp;
-                const double* pc = PS + (size_t)m * L * n2 + kx + ng * ky;
-                auto P = [&](int iz, int dx, int dy) {
-                    const int jx = dx ? mirror(kx, ng) : kx, jy = dy ? mirror(ky, ng) : ky;
-                    return pc[(size_t)iz * n2 + (jx - kx) + ng * (jy - ky)];
-                };
-                auto wka = [&](int iz, int dx, int dy) { return (P(iz + 1, dx, dy) - P(iz - 1, dx, dy)) * hdzi; };
-                auto wkd = [&](int iz, int dx, int dy) {
-                    return (P(iz + 1, dx, dy) - 2.0 * P(iz, dx, dy) + P(iz - 1, dx, dy)) * dzisq;
-                };
-                if (k == 0) return (T)((2.0 * P(0, 0, 0) - 5.0 * P(1, 0, 0) + 4.0 * P(2, 0, 0) - P(3, 0, 0)) * dzisq);
-                if (k < 4 * nz - 3) {
-                    const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
-                    if (kind == 0) return (T)(dmul(kx, ng) * wka(iz, 1, 0));
-                    if (kind == 1) return (T)(dmul(ky, ng) * wka(iz, 0, 1));
-                    if (kind == 2) return (T)wka(iz, 0, 0);
-                    return (T)wkd(iz, 0, 0);
-                }
-                // extrapolated dp/dtheta at iz = nz (spectral form of psolve.rs:232-238)
-                const int dx = (k == 4 * nz - 3), dy = !dx;
-                const double sa = wka(nz - 1, dx, dy) + dz2 * (3.0 * wkd(nz - 1, dx, dy) - wkd(nz - 2, dx, dy));
-                return (T)((dx ? dmul(kx, ng) : dmul(ky, ng)) * sa);
+                const int m = o / n3z, k = o - m * n3z, kind = k / nz, iz = k - kind * nz;
+                const double* pc = PS + (size_t)(m * L + iz) * n2;
+                if (kind == 0) return (T)pc[kx + ng * ky];
+                if (kind == 1) return (T)(dmul(kx, ng) * pc[mirror(kx, ng) + ng * ky]);
+                return (T)(dmul(ky, ng) * pc[kx + ng * mirror(ky, ng)]);
             },
             [=] __device__(int o, int iy, int ix, T val) {
-                const int m = o / nsp, k = o - m * nsp;
-                const size_t base = (size_t)m * L * n2 + iy + ng * ix;
-                if (k == 0) { D[base] = val; return; }
-                if (k < 4 * nz - 3) {
-                    const int iz = 1 + (k - 1) / 4, kind = (k - 1) & 3;
-                    T* out = kind == 0 ? A : kind == 1 ? B : kind == 2 ? C : D;
-                    out[base + (size_t)iz * n2] = val;
-                    return;
-                }
-                ((k == 4 * nz - 3) ? A : B)[base + (size_t)nz * n2] = val;
+                const int m = o / n3z, k = o - m * n3z, kind = k / nz, iz = k - kind * nz;
+                (kind == 0 ? A : kind == 1 ? B : C)[(size_t)(m * L + iz) * n2 + iy + ng * ix] = val;
             });
         // (b) total source S = S0 + S1(p), to spectral space
         fft.ptospc(st, ML,
@@ -1159,17 +1208,33 @@ struct Solver {
                 const int i = iy + ng * ix;
                 const size_t p = (size_t)q * n2 + i;
                 const size_t cb = (size_t)m * L * n2 + i;
+                auto P = [&](int l) { return l >= nz ? 0.0 : (double)A[cb + (size_t)l * n2]; };
+                auto X = [&](int l) { return l >= nz ? 0.0 : (double)B[cb + (size_t)l * n2]; };
+                auto Y = [&](int l) { return l >= nz ? 0.0 : (double)C[cb + (size_t)l * n2]; };
                 double s;
                 if (iz == 0) {
-                    s = (double)SP0[p] + (double)C2[p] * (double)D[p];
+                    const double d2 = (2.0 * P(0) - 5.0 * P(1) + 4.0 * P(2) - P(3)) * dzisq;
+                    s = (double)SP0[p] + (double)C2[p] * d2;
                 } else if (iz < nz) {
-                    s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
-                    s += (double)C2[p] * (double)D[p] + (double)C1[p] * (double)C[p];
+                    const double dxt = (X(iz + 1) - X(iz - 1)) * hdzi;
+                    const double dyt = (Y(iz + 1) - Y(iz - 1)) * hdzi;
+                    const double dpdt = (P(iz + 1) - P(iz - 1)) * hdzi;
+                    const double d2 = (P(iz + 1) - 2.0 * P(iz) + P(iz - 1)) * dzisq;
+                    s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
+                    s += (double)C2[p] * d2 + (double)C1[p] * dpdt;
                 } else {
-                    const double d1 = D[cb + (size_t)(nz - 1) * n2], d2 = D[cb + (size_t)(nz - 2) * n2];
-                    const double dpdt = (double)C[cb + (size_t)(nz - 1) * n2] + dz2 * (3.0 * d1 - d2);
+                    // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238)
+                    auto ext = [&](auto F) {
+                        const double a1 = (F(nz) - F(nz - 2)) * hdzi;
+                        const double d1 = (F(nz) - 2.0 * F(nz - 1) + F(nz - 2)) * dzisq;
+                        const double d2 = (F(nz - 1) - 2.0 * F(nz - 2) + F(nz - 3)) * dzisq;
+                        return a1 + dz2 * (3.0 * d1 - d2);
+                    };
+                    const double dxt = ext(X), dyt = ext(Y), dpdt = ext(P);
+                    const double d1 = (P(nz) - 2.0 * P(nz - 1) + P(nz - 2)) * dzisq;
+                    const double d2 = (P(nz - 1) - 2.0 * P(nz - 2) + P(nz - 3)) * dzisq;
                     const double d2pdt2 = 2.0 * d1 - d2;
-                    s = (double)SP0[p] + (double)SIGX[p] * (double)A[p] + (double)SIGY[p] * (double)B[p];
+                    s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
                     s += (double)C2[p] * d2pdt2 + (double)C1[p] * dpdt;
                 }
                 return (T)s;
@@ -1180,10 +1245,19 @@ struct Solver {
         //     applies the stop rule (psolve.rs:89, 285-358)
         const int nblk = (n2 + THOMAS_THREADS - 1) / THOMAS_THREADS;
         double* part = red_partial.p;
-        k_thomas<T><<<dim3(nblk, M), THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part);
+        {
+            const dim3 g(nblk, M);
+            switch (nz) {
+                case 4: k_thomas<T, 4><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
+                case 8: k_thomas<T, 8><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
+                case 16: k_thomas<T, 16><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
+                case 32: k_thomas<T, 32><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
+                default: k_thomas<T, 0><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
+            }
+        }
         SW_CHECK_LAUNCH();
         count_launch();
-        k_psolve_ctrl<<<1, 256, 0, st>>>(M, nblk, part, ctl, errp, toler, mixed ? 1 : 0, nitmax, use_cond ? 1 : 0,
+        k_psolve_ctrl<<<1, CTRL_THREADS, 0, st>>>(M, nblk, part, ctl, errp, toler, mixed ? 1 : 0, nitmax, use_cond ? 1 : 0,
                                          cond, sweep_exec.p);
         SW_CHECK_LAUNCH();
         count_launch();
