@@ -836,7 +836,7 @@ struct Solver {
         const double dz2 = (HBAR / (double)nz) / 2.0;
         const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
         const double qdzi = (1.0 / 4.0) * (1.0 / (HBAR / (double)nz));
-        const double *filt = op.filt, *glap = op.glap, *theta = op.theta;
+        const double *filt = op.filt, *glap = op.glap, *theta = op.theta, *rlap = op.rlap;
         const double *DS = ds, *QS = qs, *GS = gs;
         double *PS = ps, *PSA = WD(0);
         T *R = r, *U = u, *V = v, *WW = w, *Z = z, *ZX = zx, *ZY = zy, *RI = ri, *AA = aa, *ZE = zeta, *PN = pn;
@@ -844,29 +844,32 @@ struct Solver {
         T *Sr = W(0), *S1 = W(1), *SA = W(2), *SB = W(3), *Sx = W(17), *Sy = W(18), *Sc = W(19), *D = W(7);
         T *RS = W(5), *Sd = W(6), *Su = W(8), *Sv = W(9), *Sw = W(10);
         T *UX = W(11), *UY = W(12), *VX = W(13), *VY = W(14), *WX = W(15), *WY = W(16);
-        T *zd = W(20), *HZ = W(21);
+        T* HZ = W(21);
         T *Spp = W(0), *Spq = W(1), *Spr = W(2), *Pp = W(3), *Pq = W(5), *Pr = W(6), *Sq2 = W(0);
         T* hs = plane_t.p;
         T* hsrc = plane_t.p + (size_t)M * n2;
         double* hspec = plane_d.p;
-        // P0: z by trapezoidal integration (+ theta); deviation kept apart for float32
+        // P0: z by trapezoidal integration (+ theta)
         for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
             T* zc = Z + (size_t)m * L * n2 + i;
             const T* rc = R + (size_t)m * L * n2 + i;
             double prev = dz2 * ((double)rc[0] + (double)rc[n2]);
-            zc[n2] = (T)prev;
-            if (mixed) zd[(size_t)m * L * n2 + i + n2] = (T)prev;
+            zc[n2] = (T)(prev + theta[1]);
 #pragma unroll 4
             for (int iz = 1; iz < nz; iz++) {
                 prev = prev + dz2 * ((double)rc[(size_t)iz * n2] + (double)rc[(size_t)(iz + 1) * n2]);
-                zc[(size_t)(iz + 1) * n2] = (T)prev;
-                if (mixed) zd[(size_t)m * L * n2 + i + (size_t)(iz + 1) * n2] = (T)prev;
+                zc[(size_t)(iz + 1) * n2] = (T)(prev + theta[iz + 1]);
             }
-            for (int iz = 1; iz <= nz; iz++) zc[(size_t)iz * n2] = (T)((double)zc[(size_t)iz * n2] + theta[iz]);
         });
         if (mixed) {
-            // float64 spectral h deviation and vertical-mean eta (as cpsource's mixed path)
+            // The float32 path takes the spectrum of z - theta from float64 data
+            // instead of transforming float32 z: main_invert sets r = spctop(rhat)
+            // with rhat = cofi (cofi gs - qs) - <.>, so the trapezoid of rhat over the
+            // levels is exactly the spectrum of z - theta.  Transforming float32 z
+            // would put white rounding noise into z_x, z_y that the k factor of the
+            // derivative amplifies.  The same loop gives the spectral h deviation
+            // (the top level) and the vertical mean for cpsource's HZ term.
             const double *rope = op.rope, *wgt = op.weight;
             for_cols(st, M * n2, [=] __device__(int c) {
                 const int m = c / n2, i = c - m * n2;
@@ -880,17 +883,21 @@ struct Solver {
                 for (int iz = 0; iz < L; iz++) {
                     const size_t p = (size_t)(m * L + iz) * n2 + i;
                     const double wka = COFI * (COFI * GS[p] - QS[p]) - wv;
-                    if (iz > 0) h += dz2 * (prev + wka);
+                    if (iz > 0) {
+                        h += dz2 * (prev + wka);
+                        S1[p] = (T)h;
+                    }
                     prev = wka;
                 }
                 hspec[c] = h;
                 hspec[(size_t)M * n2 + c] = wv;
             });
         }
-        const T* zsrc = mixed ? zd : Z;
-        // P1: forward transforms of everything physical that is known now
-        const int o_z = ML, o_a = ML + Mnz, o_b = o_a + ML, o_p = o_b + ML, o_u = o_p + ML, o_v = o_u + ML,
-                  o_h = o_v + ML;
+        // P1: forward transforms of everything physical that is known now (z, u and
+        // v only on the float64 path: the float32 path filled S1 above and takes the
+        // u, v derivatives from float64 spectral data in P2)
+        const int o_z = ML, o_a = ML + (mixed ? 0 : Mnz), o_b = o_a + ML, o_p = o_b + ML, o_u = o_p + ML,
+                  o_v = o_u + (mixed ? 0 : ML), o_h = o_v + (mixed ? 0 : ML);
         const int n1 = o_h + (mixed ? 0 : M);
         fft.ptospc(st, n1,
             [=] __device__(int o, int iy, int ix) -> T {
@@ -898,7 +905,7 @@ struct Solver {
                 if (o < o_z) return T(1) / (R[(size_t)o * n2 + pi] + T(1));
                 if (o < o_a) {
                     const int k = o - o_z, m = k / nz, iz = 1 + k % nz;
-                    return zsrc[(size_t)(m * L + iz) * n2 + pi];
+                    return Z[(size_t)(m * L + iz) * n2 + pi];
                 }
                 if (o < o_b) { const size_t p = (size_t)(o - o_a) * n2 + pi; return U[p] * R[p]; }
                 if (o < o_p) { const size_t p = (size_t)(o - o_b) * n2 + pi; return V[p] * R[p]; }
@@ -952,6 +959,25 @@ struct Solver {
                 }
                 if (o < q_h) {
                     const int k = o - q_d, which = k / ML, q = k - which * ML;
+                    if (mixed) {
+                        // u_x, u_y, v_x, v_y straight from qs, ds, gs (main_invert's
+                        // spectral u, v differentiated once more), so float32 rounding
+                        // of the physical u, v is not amplified by the derivative.
+                        const size_t b = (size_t)q * n2;
+                        const double* wk = hspec + (size_t)M * n2 + (size_t)(q / L) * n2;
+                        const int ax_m = mirror(kx, ng), ay_m = mirror(ky, ng), i1 = ax_m + ng * ay_m;
+                        auto wkc = [&](int j) {
+                            const double e = COFI * (COFI * GS[b + j] - QS[b + j]) - wk[j];
+                            return rlap[j] * (QS[b + j] + COF * e);
+                        };
+                        const double d0 = rlap[i] * DS[b + i], d1 = rlap[i1] * DS[b + i1];
+                        const double c0 = wkc(i), c1 = wkc(i1);
+                        const double ax = dmul(kx, ng), ay = dmul(ky, ng), bx = dmul(ax_m, ng), by = dmul(ay_m, ng);
+                        if (which == 0) return (T)(ax * (bx * d0 - ay * c1));
+                        if (which == 1) return (T)(ay * (ax * d1 - by * c0));
+                        if (which == 2) return (T)(ax * (ay * d1 + bx * c0));
+                        return (T)(ay * (by * d0 + ax * c1));
+                    }
                     const T* sv = (which < 2 ? Su : Sv) + (size_t)q * n2;
                     return (which & 1) == 0 ? (T)(dmul(kx, ng) * (double)sv[mx]) : (T)(dmul(ky, ng) * (double)sv[my]);
                 }
