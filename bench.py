@@ -217,6 +217,7 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     M = args.members
     sp = sw.Spectral(NG, NZ, precision=prec, nmembers=M, device=local)
     sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
+    tune = sp.autotune() if args.autotune == "on" else None
     qq2 = sw.vstrip.pv_strip(NG)
     for m in range(M):
         q3, d3, g3 = initial_fields(NG, NZ, 1 + rank * M + m, lambda ng: qq2)
@@ -256,6 +257,7 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
         "precision": precision, "w_fft": w_fft, "ms": ms, "t_local": t_local,
         "value": replica_throughput(args.steps * M, t_local, world, "cuda"),
         "launches": int(n1.value - n0.value), "sweeps": float(np.mean(sweeps_seen)), "clocks": clk.summary(),
+        "tune": tune,
         "snapshot": {k: st.get(k).ravel(order="F") for k in ("qs", "ds", "gs", "pn")},
     }
     if full:
@@ -303,6 +305,8 @@ def main():
     ap.add_argument("--fft-only", action="store_true",
                     help="only time the batched 2-D transform pass (for profiling the top kernel)")
     ap.add_argument("--planes", type=int, default=6 * (NZ + 1))
+    ap.add_argument("--autotune", default="on", choices=["on", "off"],
+                    help="time the 2-D transform launch chunk candidates before warm-up and keep the fastest")
     ap.add_argument("--graphs", default="on", choices=["on", "off"],
                     help="run each step as one CUDA graph (on) or host-driven (off; same kernels, for profiling)")
     args = ap.parse_args()
@@ -358,7 +362,8 @@ def main():
                                    "(seed per member), delta=gamma=0",
                        "ng": NG, "nz": NZ, "members_per_gpu": M, "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
-                       "psolve_sweeps_per_step": main_arm["sweeps"]},
+                       "psolve_sweeps_per_step": main_arm["sweeps"],
+                       "fft_autotune": main_arm["tune"]},
             "e2e": main_arm["e2e"],
             "gpu_launches": main_arm["launches"],
             "roofline": {"bound": "hbm", "kernel": "k_fft_pass (batched 2-D transform pass, %d planes)"

@@ -118,6 +118,18 @@ int sw_advance(sw_ctx* ctx, int nsteps, int ggen);
  * conditional WHILE nodes (enable = 1, the default), or drive the iterations from
  * the host with one synchronisation per sweep (enable = 0).  Same results. */
 int sw_set_graphs(sw_ctx* ctx, int enable);
+/* Tuning of the batched 2-D transforms: planes per pair of tile-pass launches
+ * (1 .. the context's capacity, 6*(nz+1)*nmembers).  *in_use (may be NULL) gets
+ * the clamped value.  Results do not depend on it.  No reference counterpart:
+ * the reference transforms one plane at a time (src/sta2dfft.rs:91-123). */
+int sw_set_fft_chunk(sw_ctx* ctx, int planes, int* in_use);
+/* Autotuner of that chunk: times reps forward + inverse transforms of the
+ * pressure sweep's batch (3*nz planes per member) at each candidate (the capacity,
+ * halved down to 8 planes), on scratch buffers it allocates, and keeps the
+ * fastest.  Up to maxc rows of (chunks[i], ms[i] per transform pair) are written
+ * when the arrays are non-NULL; *ncand gets the row count, *chosen the chunk now
+ * in use.  No reference counterpart. */
+int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* chunks, float* ms, int* ncand, int* chosen);
 /* diagnose (src/nhswps/mod.rs:666-711) of one member:
  * out = {0.5*zrms^2, zrms, zmax, umax}. */
 int sw_diagnose(sw_ctx* ctx, int member, double out[4]);

@@ -64,6 +64,8 @@ _SIGS = {
     "sw_source": (_i, [_vp, _dp, _dp, _dp]),
     "sw_advance": (_i, [_vp, _i, _i]),
     "sw_set_graphs": (_i, [_vp, _i]),
+    "sw_set_fft_chunk": (_i, [_vp, _i, _ip]),
+    "sw_autotune_fft": (_i, [_vp, _i, _i, _ip, ctypes.POINTER(ctypes.c_float), _ip, _ip]),
     "sw_diagnose": (_i, [_vp, _i, _dp]),
     "sw_diag_history": (_i, [_vp, _dp, _i, _ip]),
     "sw_energy": (_i, [_vp, _i, _dp]),

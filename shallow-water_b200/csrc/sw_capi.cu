@@ -677,6 +677,21 @@ int sw_set_graphs(sw_ctx* ctx, int enable) {
         return SW_OK;
     });
 }
+int sw_set_fft_chunk(sw_ctx* ctx, int planes, int* in_use) {
+    return with_solver(ctx, [&](auto& s) {
+        const int v = s.set_fft_chunk(planes);
+        if (in_use) *in_use = v;
+        return SW_OK;
+    });
+}
+int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* chunks, float* ms, int* ncand, int* chosen) {
+    if (maxc < 0) return fail(SW_ERR_ARG, "maxc must be >= 0");
+    return with_solver(ctx, [&](auto& s) {
+        const int v = s.autotune_fft(reps, maxc, chunks, ms, ncand);
+        if (chosen) *chosen = v;
+        return SW_OK;
+    });
+}
 int sw_fft2d_dev(sw_ctx* ctx, int direction, int nplanes, const void* in, void* out) {
     return with_solver(ctx, [&](auto& s) { return sw::capi::fft2d_impl(s, direction, nplanes, in, out); });
 }

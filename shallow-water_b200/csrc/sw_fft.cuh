@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace sw {
 
 template <typename T> struct C2;
@@ -380,6 +382,165 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
             val = (c & 1) ? a.y : a.x;
         }
         st(o, col, k, val * sc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Static-length pass (n = 128 or 256, tile 1 << LTCS columns, every tile full).
+// Each thread owns column PAIRS: it loads columns (2p, 2p+1) of a point together
+// and writes them as one complex value, so index arithmetic, shared-memory
+// traffic and the Hermitian pack/unpack are done once per pair.  The reverse
+// transform packs on load: a thread takes points k and n-k of its pair and writes
+// Z[k], Z[n-k] directly.  The forward transform unpacks on store the same way,
+// producing modes k and n-k of both columns from two shared-memory reads.  Row
+// indices are affine in the compile-time loop counter, so the functors' address
+// arithmetic folds into immediate offsets.
+// ---------------------------------------------------------------------------
+
+// Functors that tag `static constexpr bool pair_io = true` provide
+// ld2(o, col, pt) -> T2 and st2(o, col, pt, a, b) for the adjacent columns
+// (col, col+1), col even; others get two scalar calls.
+template <class F, class = void>
+struct pair_io : std::false_type {};
+template <class F>
+struct pair_io<F, std::void_t<decltype(F::pair_io)>> : std::integral_constant<bool, F::pair_io> {};
+
+template <typename T, class LD>
+__device__ __forceinline__ void ld_pair(const LD& ld, int o, int col, int j, T& a, T& b) {
+    if constexpr (pair_io<LD>::value) {
+        const auto v = ld.ld2(o, col, j);
+        a = v.x;
+        b = v.y;
+    } else {
+        a = (T)ld(o, col, j);
+        b = (T)ld(o, col + 1, j);
+    }
+}
+template <typename T, class ST>
+__device__ __forceinline__ void st_pair(const ST& st, int o, int col, int k, T a, T b) {
+    if constexpr (pair_io<ST>::value) {
+        st.st2(o, col, k, a, b);
+    } else {
+        st(o, col, k, a);
+        st(o, col + 1, k, b);
+    }
+}
+
+template <typename T, int NS, int LTCS, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
+__global__ void __launch_bounds__(FFT_THREADS, 3)
+k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
+    using T2 = typename C2<T>::t;
+    static_assert(NS == 128 || NS == 256, "static lengths: 128, 256");
+    static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
+    static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
+    constexpr int N = NS, H = N / 2, TC = 1 << LTCS, NP = TC / 2, PL = N + (N >> 4) + 1, TH = FFT_THREADS;
+    constexpr int RS = TH / NP;  // rows per sweep of the pair-major mappings
+    static_assert(TH % NP == 0 && H % RS == 0, "tile and block shape");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* tw = reinterpret_cast<T2*>(smem_raw);
+    T2* buf0 = tw + N;
+    T2* buf1 = buf0 + NP * PL;
+    const int tid = threadIdx.x;
+    const int o = blockIdx.y;
+    const int c0 = blockIdx.x * TC;
+    for (int i = tid; i < N; i += TH) tw[i] = twg[i];
+
+    if constexpr (INV) {
+        // points k and n-k of pair p (k = 0 takes points 0 and n/2), packed into Z
+        constexpr int U = H / RS;
+        const int p = tid % NP, r0 = tid / NP, col = c0 + 2 * p;
+        T a1[U], b1[U], a2[U], b2[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = r0 + RS * u;
+            ld_pair<T>(ld, o, col, k, a1[u], b1[u]);
+            ld_pair<T>(ld, o, col, k == 0 ? H : N - k, a2[u], b2[u]);
+        }
+        T2* z = buf0 + p * PL;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = r0 + RS * u;
+            T2 lo, hi;
+            if (k == 0) {
+                lo.x = a1[u]; lo.y = b1[u];
+                hi.x = a2[u]; hi.y = b2[u];
+                z[pad16(0)] = lo;
+                z[pad16(H)] = hi;
+            } else {
+                lo.x = a1[u] - b2[u]; lo.y = a2[u] + b1[u];
+                hi.x = a1[u] + b2[u]; hi.y = b1[u] - a2[u];
+                z[pad16(k)] = lo;
+                z[pad16(N - k)] = hi;
+            }
+        }
+    } else if constexpr (LOAD_CF) {
+        constexpr int U = N / RS;
+        const int p = tid % NP, r0 = tid / NP, col = c0 + 2 * p;
+        T a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) ld_pair<T>(ld, o, col, r0 + RS * u, a[u], b[u]);
+        T2* z = buf0 + p * PL;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            T2 v;
+            v.x = a[u]; v.y = b[u];
+            z[pad16(r0 + RS * u)] = v;
+        }
+    } else {
+        // point-contiguous input: a warp reads 32 consecutive points of one column
+        constexpr int PS = TH / N, U = NP / PS;
+        static_assert(TH % N == 0 && NP % PS == 0, "point-major mapping");
+        const int j = tid % N, pb = tid / N;
+        T a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) ld_pair<T>(ld, o, c0 + 2 * (pb + PS * u), j, a[u], b[u]);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            T2 v;
+            v.x = a[u]; v.y = b[u];
+            buf0[(pb + PS * u) * PL + pad16(j)] = v;
+        }
+    }
+    __syncthreads();
+    const T2* Z = smem_fft_static<NS, INV>(buf0, buf1, tw, NP, PL);
+
+    if constexpr (!INV) {
+        // modes k and n-k of both columns of pair p from Z[k], Z[n-k]
+        constexpr int U = H / RS;
+        const int p = tid % NP, r0 = tid / NP, col = c0 + 2 * p;
+        const T2* z = Z + p * PL;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = r0 + RS * u;
+            if (k == 0) {
+                const T2 a = z[pad16(0)], b = z[pad16(H)];
+                st_pair<T>(st, o, col, 0, a.x * sc, a.y * sc);
+                st_pair<T>(st, o, col, H, b.x * sc, b.y * sc);
+            } else {
+                const T2 a = z[pad16(k)], b = z[pad16(N - k)];
+                st_pair<T>(st, o, col, k, T(0.5) * (a.x + b.x) * sc, T(0.5) * (a.y + b.y) * sc);
+                st_pair<T>(st, o, col, N - k, T(0.5) * (a.y - b.y) * sc, T(0.5) * (b.x - a.x) * sc);
+            }
+        }
+    } else if constexpr (STORE_CF) {
+        constexpr int U = N / RS;
+        const int p = tid % NP, r0 = tid / NP, col = c0 + 2 * p;
+        const T2* z = Z + p * PL;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = r0 + RS * u;
+            const T2 a = z[pad16(k)];
+            st_pair<T>(st, o, col, k, a.x * sc, a.y * sc);
+        }
+    } else {
+        constexpr int PS = TH / N, U = NP / PS;
+        const int j = tid % N, pb = tid / N;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int p = pb + PS * u;
+            const T2 a = Z[p * PL + pad16(j)];
+            st_pair<T>(st, o, c0 + 2 * p, j, a.x * sc, a.y * sc);
+        }
     }
 }
 

@@ -37,13 +37,25 @@ struct MidPC {
     __device__ __forceinline__ T operator()(int o, int c, int p) const { return m[((size_t)o * ng + c) * ng + p]; }
     __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { m[((size_t)o * ng + c) * ng + p] = v; }
 };
-// intermediate addressed [col + ng*pt] (column index contiguous)
+// intermediate addressed [col + ng*pt] (column index contiguous); columns
+// (c, c+1), c even, are one aligned vector access
 template <typename T>
 struct MidCP {
+    using T2 = typename C2<T>::t;
+    static constexpr bool pair_io = true;
     T* m;
     int ng;
     __device__ __forceinline__ T operator()(int o, int c, int p) const { return m[((size_t)o * ng + p) * ng + c]; }
     __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { m[((size_t)o * ng + p) * ng + c] = v; }
+    __device__ __forceinline__ T2 ld2(int o, int c, int p) const {
+        return *reinterpret_cast<const T2*>(m + ((size_t)o * ng + p) * ng + c);
+    }
+    __device__ __forceinline__ void st2(int o, int c, int p, T a, T b) const {
+        T2 v;
+        v.x = a;
+        v.y = b;
+        *reinterpret_cast<T2*>(m + ((size_t)o * ng + p) * ng + c) = v;
+    }
 };
 
 inline int build_plan(int n, FftPlan& plan) {
@@ -111,20 +123,37 @@ template <typename T, bool INV, bool LCF, bool SCF, class LD, class ST>
 inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T>::t* tw, int tc, T sc,
                         int nout, int ncols, LD ld, ST st) {
     if (nout <= 0) return;
-    // compile-time kernels for the common lengths when the tile matches
     constexpr int LT256 = sizeof(T) == 8 ? 4 : 5, LT128 = 5;
-    auto kern = k_fft_pass<T, 0, 0, INV, LCF, SCF, LD, ST>;
-    if (plan.n == 256 && tc == (1 << LT256)) kern = k_fft_pass<T, 256, LT256, INV, LCF, SCF, LD, ST>;
-    else if (plan.n == 128 && tc == (1 << LT128)) kern = k_fft_pass<T, 128, LT128, INV, LCF, SCF, LD, ST>;
     const size_t smem = fft_pass_smem<T>(plan.n, tc);
-    static int attr_done[64][3] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int kv = plan.n == 256 ? 1 : plan.n == 128 ? 2 : 0;
-    if (dev < 64 && !attr_done[dev][kv]) {
+    // compile-time pair kernels for the common lengths when the tile matches and
+    // every tile is full (the generic kernel covers the rest)
+    constexpr bool pair_ok = INV ? LCF : SCF;
+    if constexpr (pair_ok) {
+        const bool s256 = plan.n == 256 && tc == (1 << LT256), s128 = plan.n == 128 && tc == (1 << LT128);
+        if ((s256 || s128) && ncols % tc == 0) {
+            auto kern = s256 ? k_fft_pass_s<T, 256, LT256, INV, LCF, SCF, LD, ST>
+                             : k_fft_pass_s<T, 128, LT128, INV, LCF, SCF, LD, ST>;
+            static int attr_s[64][2] = {};
+            if (dev < 64 && !attr_s[dev][s256 ? 0 : 1]) {
+                SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+                SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+                attr_s[dev][s256 ? 0 : 1] = 1;
+            }
+            dim3 grid(ncols / tc, nout);
+            kern<<<grid, FFT_THREADS, smem, s>>>(tw, sc, ld, st);
+            SW_CHECK_LAUNCH();
+            count_launch();
+            return;
+        }
+    }
+    auto kern = k_fft_pass<T, 0, 0, INV, LCF, SCF, LD, ST>;
+    static int attr_done[64] = {};
+    if (dev < 64 && !attr_done[dev]) {
         SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        attr_done[dev][kv] = 1;
+        attr_done[dev] = 1;
     }
     dim3 grid((ncols + tc - 1) / tc, nout);
     kern<<<grid, FFT_THREADS, smem, s>>>(plan, tw, ncols, ilog2(tc), make_fastdiv((uint32_t)plan.n), sc, ld, st);
@@ -139,9 +168,18 @@ struct Fft2d {
     FftPlan plan{};
     DevBuf<T2> tw;
     DevBuf<T> mid;
-    int cap = 0;  // planes the intermediate holds
+    int cap = 0;    // planes the intermediate holds
+    int chunk = 0;  // planes per pair of pass launches (<= cap)
     int tc = 2;
     T sc = 1;
+
+    // Default chunk: the intermediate of one launch pair stays within about 40 MB,
+    // a third of the 126 MB L2, so that pass B reads what pass A wrote from L2.
+    static int default_chunk(int ng, int cap) {
+        const size_t plane = (size_t)ng * ng * sizeof(T);
+        const int c = (int)((40u << 20) / plane);
+        return c < 1 ? 1 : (c > cap ? cap : c);
+    }
 
     void init(int ng_, int cap_planes) {
         ng = ng_;
@@ -151,22 +189,28 @@ struct Fft2d {
         SW_CUDA(cudaMemcpy(tw.p, h.data(), sizeof(T2) * ng, cudaMemcpyHostToDevice));
         cap = cap_planes;
         mid.alloc((size_t)cap * ng * ng);
+        chunk = default_chunk(ng, cap);
         tc = pick_tile<T>(ng);
         sc = (T)(1.0 / std::sqrt((double)ng));
+    }
+    // Planes per launch pair, clamped to [1, cap]; returns the value in use.
+    int set_chunk(int planes) {
+        chunk = planes < 1 ? 1 : (planes > cap ? cap : planes);
+        return chunk;
     }
 
     template <class LD, class ST>
     void spctop(cudaStream_t s, int nout, LD ld, ST st) const {
-        for (int o0 = 0; o0 < nout; o0 += cap) {
-            const int cnt = (nout - o0 < cap) ? nout - o0 : cap;
+        for (int o0 = 0; o0 < nout; o0 += chunk) {
+            const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
             launch_pass<T, true, true, false>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidPC<T>{mid.p, ng});
             launch_pass<T, true, true, true>(s, plan, tw.p, tc, sc, cnt, ng, MidCP<T>{mid.p, ng}, StOff<ST>{st, o0});
         }
     }
     template <class LD, class ST>
     void ptospc(cudaStream_t s, int nout, LD ld, ST st) const {
-        for (int o0 = 0; o0 < nout; o0 += cap) {
-            const int cnt = (nout - o0 < cap) ? nout - o0 : cap;
+        for (int o0 = 0; o0 < nout; o0 += chunk) {
+            const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
             launch_pass<T, false, true, true>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidCP<T>{mid.p, ng});
             launch_pass<T, false, false, true>(s, plan, tw.p, tc, sc, cnt, ng, MidPC<T>{mid.p, ng}, StOff<ST>{st, o0});
         }

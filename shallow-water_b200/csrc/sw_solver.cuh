@@ -40,7 +40,7 @@ template <typename T, int NZS>
 __global__ void __launch_bounds__(THOMAS_THREADS)
 k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __restrict__ SP,
          const double* __restrict__ htdv, const double* __restrict__ etdv, const double* __restrict__ ap,
-         double* __restrict__ PS, double* __restrict__ PSA, double* __restrict__ part) {
+         double* __restrict__ PS, double* __restrict__ XF, double* __restrict__ part) {
     const int m = blockIdx.y;
     const int i = blockIdx.x * THOMAS_THREADS + threadIdx.x;
     const int nz = NZS ? NZS : nz_rt;
@@ -63,19 +63,17 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
 #pragma unroll
         for (int iz = 0; iz < NZS; iz++) {
             const size_t p = cb + (size_t)iz * n2;
-            const double old = PSA[p];
+            const double old = PS[p];
             sn += (x[iz] - old) * (x[iz] - old);
             sd += old * old;
             PS[p] = x[iz];
-            PSA[p] = x[iz];
         }
         {
             const size_t p = cb + (size_t)NZS * n2;
-            const double old = PSA[p];
+            const double old = PS[p];
             sn += old * old;
             sd += old * old;
             PS[p] = 0.0;
-            PSA[p] = 0.0;
         }
         const int kx = i % ng, ky = i / ng;
         const double wgt = pweight(kx, ng) * pweight(ky, ng);
@@ -86,41 +84,39 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
         const double api = ap[i];
         double spm = (double)SP[cb], spc = (double)SP[cb + n2];
         double x = ((1.0 / 3.0) * spm + (1.0 / 6.0) * spc) * htdv[i];
-        PS[cb] = x;
+        XF[cb] = x;
 #pragma unroll 4
         for (int iz = 1; iz < nz; iz++) {
             const double spp = (double)SP[cb + (size_t)(iz + 1) * n2];
             const double g = (1.0 / 12.0) * (spm + spp) + (5.0 / 6.0) * spc;
             x = (g - api * x) * htdv[i + (size_t)n2 * iz];
-            PS[cb + (size_t)iz * n2] = x;
+            XF[cb + (size_t)iz * n2] = x;
             spm = spc;
             spc = spp;
         }
         {
             const size_t p = cb + (size_t)nz * n2;
-            const double old = PSA[p];
+            const double old = PS[p];
             sn += old * old;
             sd += old * old;
             PS[p] = 0.0;
-            PSA[p] = 0.0;
         }
         double xn = x;
         {
             const size_t p = cb + (size_t)(nz - 1) * n2;
-            const double old = PSA[p];
+            const double old = PS[p];
             sn += (xn - old) * (xn - old);
             sd += old * old;
-            PSA[p] = xn;
+            PS[p] = xn;
         }
 #pragma unroll 4
         for (int iz = nz - 2; iz >= 0; iz--) {
             const size_t p = cb + (size_t)iz * n2;
-            const double xi = PS[p] + etdv[i + (size_t)n2 * iz] * xn;
-            const double old = PSA[p];
+            const double xi = XF[p] + etdv[i + (size_t)n2 * iz] * xn;
+            const double old = PS[p];
             sn += (xi - old) * (xi - old);
             sd += old * old;
             PS[p] = xi;
-            PSA[p] = xi;
             xn = xi;
         }
         const int kx = i % ng, ky = i / ng;
@@ -313,6 +309,79 @@ struct Solver {
         if (st_body) cudaStreamDestroy(st_body);
         if (h_pinned) cudaFreeHost(h_pinned);
         if (st) cudaStreamDestroy(st);
+    }
+
+    // Planes per 2-D transform launch pair; the captured step graphs hold the old
+    // launch sequence, so they are dropped and re-captured on the next step.
+    int set_fft_chunk(int planes) {
+        SW_CUDA(cudaStreamSynchronize(st));
+        for (auto& e : step_exec)
+            if (e) {
+                SW_CUDA(cudaGraphExecDestroy(e));
+                e = nullptr;
+            }
+        return fft.set_chunk(planes);
+    }
+
+    // Autotuner of the 2-D transform launches: times `reps` forward + inverse
+    // transforms of the pressure sweep's batch (3*nz planes per member) at each
+    // candidate chunk (cap, cap/2, ... down to 8 planes) with CUDA events on the
+    // context's stream, and keeps the fastest.  The batch runs on scratch buffers
+    // allocated for the measurement.  Writes up to maxc (chunk, ms per transform
+    // pair) rows and returns the chosen chunk.
+    int autotune_fft(int reps, int maxc, int* cand, float* ms, int* ncand) {
+        if (reps < 1) reps = 1;
+        const int nb = std::min(fft.cap, 3 * nz * M);
+        DevBuf<T> a, b;
+        a.alloc((size_t)nb * n2);
+        b.alloc((size_t)nb * n2);
+        SW_CUDA(cudaMemsetAsync(a.p, 0, sizeof(T) * (size_t)nb * n2, st));
+        const int ng = this->ng;
+        T *A = a.p, *B = b.p;
+        cudaEvent_t e0, e1;
+        SW_CUDA(cudaEventCreate(&e0));
+        SW_CUDA(cudaEventCreate(&e1));
+        std::vector<int> cands;
+        for (int c = fft.cap;; c /= 2) {
+            cands.push_back(c);
+            if (c / 2 < 8) break;
+        }
+        int best = fft.chunk, k = 0;
+        float best_ms = 1e30f;
+        try {
+            for (int c : cands) {
+                set_fft_chunk(c);
+                for (int r = -1; r < reps; r++) {  // r = -1: untimed warm-up
+                    if (r == 0) SW_CUDA(cudaEventRecord(e0, st));
+                    fft.ptospc(st, nb, [=] __device__(int o, int iy, int ix) -> T { return A[((size_t)o * ng + ix) * ng + iy]; },
+                               [=] __device__(int o, int kx, int ky, T v) { B[((size_t)o * ng + ky) * ng + kx] = v; });
+                    fft.spctop(st, nb, [=] __device__(int o, int kx, int ky) -> T { return B[((size_t)o * ng + ky) * ng + kx]; },
+                               [=] __device__(int o, int iy, int ix, T v) { A[((size_t)o * ng + ix) * ng + iy] = v; });
+                }
+                SW_CUDA(cudaEventRecord(e1, st));
+                SW_CUDA(cudaEventSynchronize(e1));
+                float t = 0.f;
+                SW_CUDA(cudaEventElapsedTime(&t, e0, e1));
+                t /= (float)(reps > 0 ? reps : 1);
+                if (k < maxc) {
+                    if (cand) cand[k] = fft.chunk;
+                    if (ms) ms[k] = t;
+                }
+                k++;
+                if (t < best_ms) {
+                    best_ms = t;
+                    best = fft.chunk;
+                }
+            }
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (ncand) *ncand = k < maxc ? k : maxc;
+        return set_fft_chunk(best);
     }
 
     T* W(int i) { return wt[i].p; }
@@ -763,7 +832,9 @@ struct Solver {
     // ======================================================================
     // psolve (src/nhswps/psolve.rs:16-411)
     // Work: W(0..3) A,B,C,D physical sweep terms; W(4) sp (spectral source);
-    // WD(0) psa (previous spectral pressure), WD(1) compact RHS for dp/dtheta.
+    // PS holds the previous iterate until the Thomas kernel replaces it; WD(1) is the
+    // forward-elimination scratch of the streamed Thomas path and, after the loop,
+    // the compact RHS for dp/dtheta.
     // ctrl: [active, iters, status] per member; errp_d: errp per member.
     // Returns member-0 status.
     // ======================================================================
@@ -803,18 +874,14 @@ struct Solver {
         cpsource();
         T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
         T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
-        double* PSA = WD(0);
         int* ctl = ctrl.p;
         double* errp = errp_d.p;
-        // spectral pressure of the first guess: psa = ptospc(pn) (all levels), ps = psa with ps(nz) = 0
+        // spectral pressure of the first guess, all levels: ps = ptospc(pn).  The sweep
+        // reads levels 0..nz-1 only (ps(nz) = 0 in psolve.rs); the first Thomas solve
+        // takes ps(nz) into the residual as the previous iterate and then zeroes it.
         fft.ptospc(st, ML,
             [=] __device__(int q, int iy, int ix) -> T { return PN[(size_t)q * n2 + iy + ng * ix]; },
-            [=] __device__(int q, int kx, int ky, T val) {
-                const int iz = q % L;
-                const size_t p = (size_t)q * n2 + kx + ng * ky;
-                PSA[p] = (double)val;
-                PS[p] = (iz == nz) ? 0.0 : (double)val;
-            });
+            [=] __device__(int q, int kx, int ky, T val) { PS[(size_t)q * n2 + kx + ng * ky] = (double)val; });
         for_cols(st, M, [=] __device__(int m) {
             ctl[3 * m] = 1;
             ctl[3 * m + 1] = 0;
@@ -838,7 +905,7 @@ struct Solver {
         const double qdzi = (1.0 / 4.0) * (1.0 / (HBAR / (double)nz));
         const double *filt = op.filt, *glap = op.glap, *theta = op.theta, *rlap = op.rlap;
         const double *DS = ds, *QS = qs, *GS = gs;
-        double *PS = ps, *PSA = WD(0);
+        double* PS = ps;
         T *R = r, *U = u, *V = v, *WW = w, *Z = z, *ZX = zx, *ZY = zy, *RI = ri, *AA = aa, *ZE = zeta, *PN = pn;
         T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
         T *Sr = W(0), *S1 = W(1), *SA = W(2), *SB = W(3), *Sx = W(17), *Sy = W(18), *Sc = W(19), *D = W(7);
@@ -924,11 +991,8 @@ struct Solver {
                 }
                 if (o < o_b) { SA[(size_t)(o - o_a) * n2 + i] = val; return; }
                 if (o < o_p) { SB[(size_t)(o - o_b) * n2 + i] = val; return; }
-                if (o < o_u) {
-                    const int q = o - o_p;
-                    const size_t p = (size_t)q * n2 + i;
-                    PSA[p] = (double)val;
-                    PS[p] = (q % L == nz) ? 0.0 : (double)val;
+                if (o < o_u) {  // first-guess ps, all levels (see psolve_prepare)
+                    PS[(size_t)(o - o_p) * n2 + i] = (double)val;
                     return;
                 }
                 if (o < o_v) { Su[(size_t)(o - o_u) * n2 + i] = val; return; }
@@ -1204,7 +1268,7 @@ struct Solver {
         double* PS = ps;
         T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
         T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
-        double* PSA = WD(0);
+        double* XF = WD(1);
         int* ctl = ctrl.p;
         double* errp = errp_d.p;
         (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;
@@ -1274,11 +1338,11 @@ struct Solver {
         {
             const dim3 g(nblk, M);
             switch (nz) {
-                case 4: k_thomas<T, 4><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
-                case 8: k_thomas<T, 8><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
-                case 16: k_thomas<T, 16><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
-                case 32: k_thomas<T, 32><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
-                default: k_thomas<T, 0><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, PSA, part); break;
+                case 4: k_thomas<T, 4><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
+                case 8: k_thomas<T, 8><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
+                case 16: k_thomas<T, 16><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
+                case 32: k_thomas<T, 32><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
+                default: k_thomas<T, 0><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
             }
         }
         SW_CHECK_LAUNCH();
@@ -1302,7 +1366,6 @@ struct Solver {
         double* PS = ps;
         T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
         T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
-        double* PSA = WD(0);
         int* ctl = ctrl.p;
         double* errp = errp_d.p;
         (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;

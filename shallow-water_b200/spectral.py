@@ -58,6 +58,21 @@ class Spectral:
     def ctx(self):
         return self._ctx
 
+    def set_fft_chunk(self, planes):
+        """Planes per pair of 2-D transform launches (clamped); returns the value in use."""
+        v = ctypes.c_int()
+        check(lib().sw_set_fft_chunk(self._ctx, int(planes), ctypes.byref(v)))
+        return v.value
+
+    def autotune(self, reps=5, maxc=16):
+        """Time the candidate transform chunks on this context's grid and keep the
+        fastest.  Returns {"chosen": planes, "candidates": [(planes, ms), ...]}."""
+        chunks = (ctypes.c_int * maxc)()
+        ms = (ctypes.c_float * maxc)()
+        n, chosen = ctypes.c_int(), ctypes.c_int()
+        check(lib().sw_autotune_fft(self._ctx, int(reps), maxc, chunks, ms, ctypes.byref(n), ctypes.byref(chosen)))
+        return {"chosen": chosen.value, "candidates": [(chunks[i], float(ms[i])) for i in range(n.value)]}
+
     @property
     def n2(self):
         return self.ng * self.ng
