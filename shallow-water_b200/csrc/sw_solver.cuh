@@ -28,6 +28,78 @@ inline void upload(DevBuf<double>& d, const std::vector<double>& h) {
     SW_CUDA(cudaMemcpy(d.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
 }
 
+constexpr int UPDATE_THREADS = 128;
+
+// Semi-implicit update of one (kx, ky) column (advance.rs:60-279; the same
+// arithmetic as Solver::advance_update), LS = nz + 1 levels at compile time.  The
+// summed sources of the column stay in registers across the three vertical
+// passes, so each field is read once and qs, ds, gs are written once; the
+// summed sds, sgs are not stored (source() recomputes them before their next use).
+template <int LS, bool FIRST>
+__global__ void __launch_bounds__(UPDATE_THREADS)
+k_update(int n2, int ncols, double dt4, double dt4i, const double* __restrict__ diss,
+         const double* __restrict__ rdis, const double* __restrict__ fope, const double* __restrict__ c2g2,
+         const double* __restrict__ simp, const double* __restrict__ wgt, double* __restrict__ QS,
+         double* __restrict__ DS, double* __restrict__ GS, double* __restrict__ qsi, double* __restrict__ qsm,
+         const double* __restrict__ sqs, const double* __restrict__ sds, double* __restrict__ nds,
+         const double* __restrict__ sgs, double* __restrict__ ngs, double* __restrict__ dsi, double* __restrict__ gsi) {
+    const int c = blockIdx.x * UPDATE_THREADS + threadIdx.x;
+    if (c >= ncols) return;
+    const int m = c / n2, i = c - m * n2;
+    const size_t cb = (size_t)m * LS * n2 + i;
+    const double dis = diss[i], rd = rdis[i], fo = fope[i], cg = c2g2[i], si = simp[i];
+    double sd[LS], sg[LS];
+    double wka = 0.0, wkb = 0.0;
+#pragma unroll
+    for (int iz = 0; iz < LS; iz++) {
+        const size_t p = cb + (size_t)iz * n2;
+        const double sq = sqs[p];
+        double qi, qm, nd, ng;
+        if (FIRST) {
+            const double q = QS[p], d0 = DS[p], g0 = GS[p];
+            qi = q;
+            qm = q + dt4 * sq;
+            nd = sds[p] + dt4i * d0;
+            ng = sgs[p] + dt4i * g0;
+            qsi[p] = qi;
+            qsm[p] = qm;
+            dsi[p] = d0;
+            gsi[p] = g0;
+            nds[p] = nd;
+            ngs[p] = ng;
+        } else {
+            qi = qsi[p];
+            qm = qsm[p];
+            nd = nds[p];
+            ng = ngs[p];
+        }
+        QS[p] = dis * (qm + dt4 * sq) - qi;
+        sd[iz] = sds[p] + nd;
+        sg[iz] = sgs[p] + ng;
+        const double d = sg[iz] + rd * sd[iz];
+        wka += wgt[iz] * d;
+        wkb += wgt[iz] * sd[iz];
+    }
+    wka *= fo;
+    wkb *= cg;
+    double wkg = 0.0;
+#pragma unroll
+    for (int iz = 0; iz < LS; iz++) {
+        const size_t p = cb + (size_t)iz * n2;
+        const double d = sg[iz] + rd * sd[iz];
+        DS[p] = si * (d - wka) - dsi[p];
+        const double g = wkb - FSQ * sd[iz] + rd * sg[iz];
+        wkg += wgt[iz] * g;
+    }
+    wkg *= fo;
+#pragma unroll
+    for (int iz = 0; iz < LS; iz++) {
+        const size_t p = cb + (size_t)iz * n2;
+        const double g = wkb - FSQ * sd[iz] + rd * sg[iz];
+        GS[p] = si * (g - wkg) - gsi[p];
+    }
+}
+
 constexpr int THOMAS_THREADS = 128;
 
 // Compact fourth-order RHS and Thomas solve of one sweep (psolve.rs:285-327) for
@@ -49,32 +121,34 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
     if (NZS && i < n2 && ctl[3 * m]) {
         const size_t cb = (size_t)m * L * n2 + i;
         const double api = ap[i];
-        double sp[NZS ? NZS + 1 : 1], x[NZS ? NZS : 1];
+        // every load of the column is issued before the dependent recurrences
+        double sp[NZS ? NZS + 1 : 1], x[NZS ? NZS : 1], ed[NZS ? NZS : 1], old[NZS ? NZS + 1 : 1];
 #pragma unroll
         for (int iz = 0; iz <= NZS; iz++) sp[iz] = (double)SP[cb + (size_t)iz * n2];
-        x[0] = ((1.0 / 3.0) * sp[0] + (1.0 / 6.0) * sp[1]) * htdv[i];
+#pragma unroll
+        for (int iz = 0; iz < NZS; iz++) x[iz] = htdv[i + (size_t)n2 * iz];
+#pragma unroll
+        for (int iz = 0; iz + 1 < NZS; iz++) ed[iz] = etdv[i + (size_t)n2 * iz];
+#pragma unroll
+        for (int iz = 0; iz <= NZS; iz++) old[iz] = PS[cb + (size_t)iz * n2];
+        // forward elimination (x[iz] holds htdv(iz) until it is overwritten)
+        x[0] = ((1.0 / 3.0) * sp[0] + (1.0 / 6.0) * sp[1]) * x[0];
 #pragma unroll
         for (int iz = 1; iz < NZS; iz++) {
             const double g = (1.0 / 12.0) * (sp[iz - 1] + sp[iz + 1]) + (5.0 / 6.0) * sp[iz];
-            x[iz] = (g - api * x[iz - 1]) * htdv[i + (size_t)n2 * iz];
+            x[iz] = (g - api * x[iz - 1]) * x[iz];
         }
 #pragma unroll
-        for (int iz = NZS - 2; iz >= 0; iz--) x[iz] += etdv[i + (size_t)n2 * iz] * x[iz + 1];
+        for (int iz = NZS - 2; iz >= 0; iz--) x[iz] += ed[iz] * x[iz + 1];
 #pragma unroll
         for (int iz = 0; iz < NZS; iz++) {
-            const size_t p = cb + (size_t)iz * n2;
-            const double old = PS[p];
-            sn += (x[iz] - old) * (x[iz] - old);
-            sd += old * old;
-            PS[p] = x[iz];
+            sn += (x[iz] - old[iz]) * (x[iz] - old[iz]);
+            sd += old[iz] * old[iz];
+            PS[cb + (size_t)iz * n2] = x[iz];
         }
-        {
-            const size_t p = cb + (size_t)NZS * n2;
-            const double old = PS[p];
-            sn += old * old;
-            sd += old * old;
-            PS[p] = 0.0;
-        }
+        sn += old[NZS] * old[NZS];
+        sd += old[NZS] * old[NZS];
+        PS[cb + (size_t)NZS * n2] = 0.0;
         const int kx = i % ng, ky = i / ng;
         const double wgt = pweight(kx, ng) * pweight(ky, ng);
         sn *= wgt;
@@ -903,7 +977,7 @@ struct Solver {
         const double dz2 = (HBAR / (double)nz) / 2.0;
         const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
         const double qdzi = (1.0 / 4.0) * (1.0 / (HBAR / (double)nz));
-        const double *filt = op.filt, *glap = op.glap, *theta = op.theta, *rlap = op.rlap;
+        const double *filt = op.filt, *glap = op.glap, *theta = op.theta;
         const double *DS = ds, *QS = qs, *GS = gs;
         double* PS = ps;
         T *R = r, *U = u, *V = v, *WW = w, *Z = z, *ZX = zx, *ZY = zy, *RI = ri, *AA = aa, *ZE = zeta, *PN = pn;
@@ -960,11 +1034,10 @@ struct Solver {
                 hspec[(size_t)M * n2 + c] = wv;
             });
         }
-        // P1: forward transforms of everything physical that is known now (z, u and
-        // v only on the float64 path: the float32 path filled S1 above and takes the
-        // u, v derivatives from float64 spectral data in P2)
+        // P1: forward transforms of everything physical that is known now (z only on
+        // the float64 path; the float32 path filled S1 above)
         const int o_z = ML, o_a = ML + (mixed ? 0 : Mnz), o_b = o_a + ML, o_p = o_b + ML, o_u = o_p + ML,
-                  o_v = o_u + (mixed ? 0 : ML), o_h = o_v + (mixed ? 0 : ML);
+                  o_v = o_u + ML, o_h = o_v + ML;
         const int n1 = o_h + (mixed ? 0 : M);
         fft.ptospc(st, n1,
             [=] __device__(int o, int iy, int ix) -> T {
@@ -1023,25 +1096,6 @@ struct Solver {
                 }
                 if (o < q_h) {
                     const int k = o - q_d, which = k / ML, q = k - which * ML;
-                    if (mixed) {
-                        // u_x, u_y, v_x, v_y straight from qs, ds, gs (main_invert's
-                        // spectral u, v differentiated once more), so float32 rounding
-                        // of the physical u, v is not amplified by the derivative.
-                        const size_t b = (size_t)q * n2;
-                        const double* wk = hspec + (size_t)M * n2 + (size_t)(q / L) * n2;
-                        const int ax_m = mirror(kx, ng), ay_m = mirror(ky, ng), i1 = ax_m + ng * ay_m;
-                        auto wkc = [&](int j) {
-                            const double e = COFI * (COFI * GS[b + j] - QS[b + j]) - wk[j];
-                            return rlap[j] * (QS[b + j] + COF * e);
-                        };
-                        const double d0 = rlap[i] * DS[b + i], d1 = rlap[i1] * DS[b + i1];
-                        const double c0 = wkc(i), c1 = wkc(i1);
-                        const double ax = dmul(kx, ng), ay = dmul(ky, ng), bx = dmul(ax_m, ng), by = dmul(ay_m, ng);
-                        if (which == 0) return (T)(ax * (bx * d0 - ay * c1));
-                        if (which == 1) return (T)(ay * (ax * d1 - by * c0));
-                        if (which == 2) return (T)(ax * (ay * d1 + bx * c0));
-                        return (T)(ay * (by * d0 + ax * c1));
-                    }
                     const T* sv = (which < 2 ? Su : Sv) + (size_t)q * n2;
                     return (which & 1) == 0 ? (T)(dmul(kx, ng) * (double)sv[mx]) : (T)(dmul(ky, ng) * (double)sv[my]);
                 }
@@ -1680,6 +1734,28 @@ struct Solver {
         double *QS = qs, *DS = ds, *GS = gs;
         double *qsi = WD(2), *qsm = WD(3), *sqs = WD(4), *sds = WD(5), *nds = WD(6), *sgs = WD(7), *ngs = WD(8),
                *dsi = WD(9), *gsi = WD(10);
+        const int ncols = M * n2, nb = (ncols + UPDATE_THREADS - 1) / UPDATE_THREADS;
+#define SW_UPDATE_CASE(LSV)                                                                                      \
+    case LSV:                                                                                                    \
+        if (first)                                                                                               \
+            k_update<LSV, true><<<nb, UPDATE_THREADS, 0, st>>>(n2, ncols, dt4, dt4i, diss, rdis, fope, c2g2, simp, \
+                                                               wgt, QS, DS, GS, qsi, qsm, sqs, sds, nds, sgs, ngs,  \
+                                                               dsi, gsi);                                          \
+        else                                                                                                     \
+            k_update<LSV, false><<<nb, UPDATE_THREADS, 0, st>>>(n2, ncols, dt4, dt4i, diss, rdis, fope, c2g2,      \
+                                                                simp, wgt, QS, DS, GS, qsi, qsm, sqs, sds, nds, sgs, \
+                                                                ngs, dsi, gsi);                                     \
+        SW_CHECK_LAUNCH();                                                                                       \
+        count_launch();                                                                                          \
+        return;
+        switch (L) {
+            SW_UPDATE_CASE(5)
+            SW_UPDATE_CASE(9)
+            SW_UPDATE_CASE(17)
+            SW_UPDATE_CASE(33)
+            default: break;
+        }
+#undef SW_UPDATE_CASE
         for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
             const size_t cb = (size_t)m * L * n2 + i;
