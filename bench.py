@@ -142,8 +142,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "nhswps advance, ng=256 nz=16, batched ensemble, vstrip + N(0,1e-3) q "
-                               "(seed per member), delta=gamma=0",
+        "config": {"workload": "nhswps advance, ng=%d nz=%d, batched ensemble, vstrip + N(0,1e-3) q "
+                               "(seed per member), delta=gamma=0" % (NG, NZ),
                    "ng": NG, "nz": NZ, "members_per_gpu": args.members, "precision": "fp64",
                    "note": "CPU members run one after another, so member-steps/s is the one-member rate"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
@@ -180,6 +180,7 @@ def time_fft_pass(sw, sp, planes, w_fft, reps=20):
     sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(stream_ptr)))
     stream = torch.cuda.ExternalStream(stream_ptr.value)
     dt = torch.float64 if w_fft == 8 else torch.float32
+    planes = min(planes, sp.set_fft_chunk(planes))  # one launch per pass
     fbuf = torch.randn(planes * NG * NG, dtype=dt, device="cuda")
     obuf = torch.empty_like(fbuf)
     torch.cuda.synchronize()
@@ -289,7 +290,135 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     return res
 
 
+def drift(sw, args, rank, local):
+    """Energy and PV drift of one member over args.drift steps, FP64 and mixed.
+
+    Every 50 steps: the savegrid energies (ekin, epot, etot) and the domain-mean
+    PV anomaly of each level (the k = 0 mode of qs, which the spectral update
+    conserves: diss(0) = 1).  Reports the relative drift of etot (hyperdiffusion
+    dissipates energy, so the FP64 drift is the physical reference for the mixed
+    one), the largest change of the mean PV, and the final mixed-vs-FP64
+    differences."""
+    if rank != 0:
+        return 0
+    import torch
+    L = sw._native.lib()
+    qq2 = sw.vstrip.pv_strip(NG)
+    q3, d3, g3 = initial_fields(NG, NZ, 1, lambda ng: qq2)
+    out = {"mode": "drift", "workload": "nhswps, one member, ng=%d nz=%d, vstrip + N(0,1e-3) q, delta=gamma=0"
+                                         % (NG, NZ), "steps": args.drift, "ng": NG, "nz": NZ}
+    finals = {}
+    for prec_name, prec in (("fp64", sw.SW_FP64), ("mixed", sw.SW_MIXED)):
+        sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+        st = sw.nhswps.initial_state(sp, q3, d3, g3)
+        sw.nhswps.psolve(st)  # z, w and p of the initial state, so that its energies are complete
+        rec = []
+        t0 = time.perf_counter()
+        done = 0
+        while True:
+            e = sw.nhswps.energy(st)
+            qs = st.get("qs")
+            rec.append((done, float(e[2]), [float(qs[0, 0, iz]) for iz in range(NZ + 1)], float(e[0]), float(e[1])))
+            if done >= args.drift:
+                break
+            n = min(50, args.drift - done)
+            sw._native.check(L.sw_advance(sp.ctx, n, 1))
+            done += n
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e0 = rec[0][1]
+        pv0 = np.array(rec[0][2])
+        pvmax = max(float(np.max(np.abs(np.array(r[2]) - pv0))) for r in rec)
+        out[prec_name] = {
+            "etot_start": e0, "etot_end": rec[-1][1], "etot_rel_drift": (rec[-1][1] - e0) / e0,
+            "etot_max_rel_dev": max(abs(r[1] - e0) for r in rec) / abs(e0),
+            "ekin_end": rec[-1][3], "epot_end": rec[-1][4],
+            "pv_mean_max_abs_change": pvmax, "pv_mean_scale": float(np.max(np.abs(pv0))) if np.any(pv0) else 0.0,
+            "wall_s": wall, "steps_per_s": args.drift / wall,
+            "etot_every_50": [r[1] for r in rec],
+        }
+        finals[prec_name] = {k: st.get(k).ravel(order="F") for k in ("qs", "ds", "gs")}
+        sp.close()
+    out["mixed_vs_fp64_after"] = {k: float(np.linalg.norm(finals["mixed"][k] - finals["fp64"][k]) /
+                                          max(np.linalg.norm(finals["fp64"][k]), 1e-300)) for k in ("qs", "ds", "gs")}
+    out["etot_mixed_minus_fp64_rel"] = (out["mixed"]["etot_end"] - out["fp64"]["etot_end"]) / abs(out["fp64"]["etot_end"])
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def uneven(sw, args, rank, world, local):
+    """Ensemble of members with uneven grids: ng from {64, 96, 128, 192, 256}, nz
+    from {4, 8, 16}, drawn with a fixed seed.  Members of one (ng, nz) share one
+    batched context (one CUDA graph per step); the contexts' streams run
+    concurrently.  The timed region starts from one event that every context
+    stream waits on and ends when all of them have finished (CUDA events)."""
+    import torch
+    L = sw._native.lib()
+    rng = np.random.default_rng(2024 + rank)
+    draws = [(int(rng.choice([64, 96, 128, 192, 256])), int(rng.choice([4, 8, 16]))) for _ in range(args.uneven)]
+    groups = {}
+    for k, key in enumerate(draws):
+        groups.setdefault(key, []).append(k)
+    prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
+    ctxs = []
+    for (ng, nz), members in sorted(groups.items()):
+        sp = sw.Spectral(ng, nz, precision=prec, nmembers=len(members), device=local)
+        qq2 = sw.vstrip.pv_strip(ng)
+        for j, k in enumerate(members):
+            q3, d3, g3 = initial_fields(ng, nz, 100 + k, lambda n: qq2)
+            sw.nhswps.initial_state(sp, q3, d3, g3, member=j, invert=False)
+        sw.nhswps.main_invert_all(sp)
+        if args.autotune == "on":
+            sp.autotune()
+        sptr = ctypes.c_void_p()
+        sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(sptr)))
+        ctxs.append((ng, nz, len(members), sp, torch.cuda.ExternalStream(sptr.value)))
+    for sp in [c[3] for c in ctxs]:
+        sw._native.check(L.sw_advance_async(sp.ctx, args.warmup, 1))
+    for sp in [c[3] for c in ctxs]:
+        sw._native.check(L.sw_sync(sp.ctx))
+    torch.cuda.synchronize()
+    main = torch.cuda.current_stream()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(main)
+        ends = []
+        for ng, nz, cnt, sp, s in ctxs:
+            s.wait_event(start)
+            sw._native.check(L.sw_advance_async(sp.ctx, args.steps, 1))
+            e = torch.cuda.Event()
+            e.record(s)
+            ends.append(e)
+        for e in ends:
+            main.wait_event(e)
+        stop.record(main)
+        for sp in [c[3] for c in ctxs]:
+            sw._native.check(L.sw_sync(sp.ctx))
+        torch.cuda.synchronize()
+    secs = start.elapsed_time(stop) / 1e3
+    secs = max_over_ranks(secs, world, "cuda")
+    points = sum(cnt * ng * ng * (nz + 1) for ng, nz, cnt, _, _ in ctxs)
+    if rank == 0:
+        line = {
+            "metric": "member-steps/s, uneven ensemble", "value": world * args.uneven * args.steps / secs,
+            "unit": "member-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
+            "dtype": "f64" if prec == sw.SW_FP64 else "f32+f64", "data": "synthetic",
+            "config": {"workload": "uneven ensemble: %d members, ng in {64,96,128,192,256}, nz in {4,8,16} "
+                                   "(seeded draw), vstrip + N(0,1e-3) q per member" % args.uneven,
+                       "groups": [{"ng": ng, "nz": nz, "members": cnt} for ng, nz, cnt, _, _ in ctxs],
+                       "precision": args.precision},
+            "grid_point_steps_per_s": world * points * args.steps / secs,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    for c in ctxs:
+        c[3].close()
+    return 0
+
+
 def main():
+    global NG, NZ, METRIC
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -304,12 +433,24 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fft-only", action="store_true",
                     help="only time the batched 2-D transform pass (for profiling the top kernel)")
-    ap.add_argument("--planes", type=int, default=6 * (NZ + 1))
+    ap.add_argument("--planes", type=int, default=None, help="planes of the --fft-only pass (default 6*(nz+1))")
+    ap.add_argument("--ng", type=int, default=NG, help="horizontal grid (the headline workload is 256)")
+    ap.add_argument("--nz", type=int, default=NZ, help="layers (the headline workload is 16)")
+    ap.add_argument("--drift", type=int, default=0, metavar="STEPS",
+                    help="instead of timing: run one member STEPS steps in FP64 and in the mixed path and "
+                         "report energy and PV drift")
+    ap.add_argument("--uneven", type=int, default=0, metavar="MEMBERS",
+                    help="time an ensemble of MEMBERS members with ng drawn from {64,96,128,192,256} and nz "
+                         "from {4,8,16}: one batched context per (ng, nz) group, groups run concurrently")
     ap.add_argument("--autotune", default="on", choices=["on", "off"],
                     help="time the 2-D transform launch chunk candidates before warm-up and keep the fastest")
     ap.add_argument("--graphs", default="on", choices=["on", "off"],
                     help="run each step as one CUDA graph (on) or host-driven (off; same kernels, for profiling)")
     args = ap.parse_args()
+    NG, NZ = args.ng, args.nz
+    METRIC = "member-steps/s at ng=%d nz=%d" % (NG, NZ)
+    if args.planes is None:
+        args.planes = 6 * (NZ + 1)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -328,6 +469,10 @@ def main():
         prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
         sp = sw.Spectral(NG, NZ, precision=prec, nmembers=1, device=local)
         return fft_only(sw, sp, args, 8 if prec == sw.SW_FP64 else 4)
+    if args.drift:
+        return drift(sw, args, rank, local)
+    if args.uneven:
+        return uneven(sw, args, rank, world, local)
 
     main_arm = run_arm(sw, args, args.precision, rank, world, local, full=True)
     other = None
@@ -350,16 +495,16 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, dt = oracle_sample(1)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "1 advance step at ng=256 nz=16 (one member) of the FP64 C restatement "
-                         "(OpenMP over levels); %.1f s" % dt}
+               "sample": "1 advance step at ng=%d nz=%d (one member) of the FP64 C restatement "
+                         "(OpenMP over levels); %.1f s" % (NG, NZ, dt)}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": main_arm["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": main_arm["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w_fft == 8 else "f32+f64", "data": "synthetic",
-            "config": {"workload": "nhswps advance, ng=256 nz=16, batched ensemble, vstrip + N(0,1e-3) q "
-                                   "(seed per member), delta=gamma=0",
+            "config": {"workload": "nhswps advance, ng=%d nz=%d, batched ensemble, vstrip + N(0,1e-3) q "
+                                   "(seed per member), delta=gamma=0" % (NG, NZ),
                        "ng": NG, "nz": NZ, "members_per_gpu": M, "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
                        "psolve_sweeps_per_step": main_arm["sweeps"],

@@ -140,7 +140,15 @@ int sw_diag_history(sw_ctx* ctx, double* out, int cap, int* count);
 int sw_energy(sw_ctx* ctx, int member, double out[3]);
 /* psolve sweep counts of the last advance step for member 0 (3 entries). */
 int sw_last_sweeps(sw_ctx* ctx, int out[3]);
-/* Synchronise the context's stream. */
+/* advance without waiting: queues nsteps graph-captured steps on the context's
+ * stream and returns (with graphs off it runs them synchronously).  Contexts on
+ * different streams then run concurrently, e.g. the groups of an ensemble with
+ * uneven grid sizes.  sw_sync waits for them and returns the pressure solves'
+ * status; other calls on the context are ordered after the queued steps.  No
+ * reference counterpart (the reference runs one member). */
+int sw_advance_async(sw_ctx* ctx, int nsteps, int ggen);
+/* Synchronise the context's stream; after sw_advance_async, finish those steps
+ * and return their status (as sw_advance would). */
 int sw_sync(sw_ctx* ctx);
 
 /* ---- device-resident access for benchmarking and zero-copy callers ----------------- */

@@ -644,8 +644,27 @@ int sw_last_sweeps(sw_ctx* ctx, int out[3]) {
         return SW_OK;
     });
 }
+int sw_advance_async(sw_ctx* ctx, int nsteps, int ggen) {
+    return with_solver(ctx, [&](auto& s) {
+        require(nsteps >= 0, SW_ERR_ARG, "nsteps must be >= 0");
+        if (!s.use_graphs) {  // host-driven steps synchronise per sweep anyway
+            int st = s.advance(nsteps, ggen != 0);
+            if (st == SW_ERR_PSOLVE_DIVERGED) return fail(st, "Pressure error too large!");
+            if (st == SW_ERR_PSOLVE_MAXITER) return fail(st, "Exceeded maximum number of iterations to find pressure!");
+            return st;
+        }
+        s.advance_enqueue(nsteps, ggen != 0);
+        return SW_OK;
+    });
+}
 int sw_sync(sw_ctx* ctx) {
     return with_solver(ctx, [&](auto& s) {
+        if (s.pending) {
+            int st = s.advance_finish();
+            if (st == SW_ERR_PSOLVE_DIVERGED) return fail(st, "Pressure error too large!");
+            if (st == SW_ERR_PSOLVE_MAXITER) return fail(st, "Exceeded maximum number of iterations to find pressure!");
+            return st;
+        }
         SW_CUDA(cudaStreamSynchronize(s.st));
         return SW_OK;
     });

@@ -544,4 +544,142 @@ k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Register-staged pass for n = 256 = 16 x 16 with 16 column pairs per tile (the
+// float32 tile): 256 threads, one radix-16 butterfly each per stage.  The
+// butterfly next to global memory runs on registers: a forward pass loads the 16
+// points j + 16 r of its pair straight into the first butterfly, and a reverse
+// pass stores the 16 modes j + 16 r of its second butterfly straight to global
+// memory, so one shared-memory round trip and one barrier fewer than the
+// two-buffer pass.  The stage that stays in shared memory works in place (each
+// thread reads and writes its own 16 slots), so one tile buffer suffices.
+// ---------------------------------------------------------------------------
+constexpr int FFT_R_N = 256, FFT_R_NP = 16, FFT_R_PL = 256 + 16 + 1;
+
+template <typename T>
+inline size_t fft_pass_smem_r() {
+    return sizeof(typename C2<T>::t) * ((size_t)FFT_R_N + (size_t)FFT_R_NP * FFT_R_PL);
+}
+
+// Second radix-16 stage of 256 = 16 x 16 on the slots j + 16 r of one sequence:
+// twiddles exp(-+2 pi i r j / 256), then the butterfly; natural order in and out.
+template <bool INV, typename T2>
+__device__ __forceinline__ void stage2_16x16(T2* v, const T2* __restrict__ tw, int j) {
+#pragma unroll
+    for (int r = 1; r < 16; r++) {
+        T2 w = tw[r * j];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+    }
+    butterfly<16, INV>(v);
+}
+
+template <typename T, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
+__global__ void __launch_bounds__(FFT_THREADS, 3)
+k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
+    using T2 = typename C2<T>::t;
+    static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
+    static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
+    constexpr int N = FFT_R_N, H = N / 2, NP = FFT_R_NP, PL = FFT_R_PL, TC = 2 * NP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* tw = reinterpret_cast<T2*>(smem_raw);
+    T2* buf = tw + N;
+    const int tid = threadIdx.x;
+    const int o = blockIdx.y;
+    const int c0 = blockIdx.x * TC;
+    tw[tid] = twg[tid];
+    // (pair, butterfly) with the pair index on the lanes (column-contiguous global
+    // access) or the butterfly index on the lanes (point-contiguous access, and the
+    // conflict-free order of the in-place shared-memory stage)
+    const int pl_ = tid % NP, jl = tid / NP;  // pair-major
+    const int pp = tid / 16, jp = tid % 16;   // point-major
+
+    if constexpr (!INV) {
+        const int p = LOAD_CF ? pl_ : pp, j = LOAD_CF ? jl : jp, col = c0 + 2 * p;
+        T2 v[16];
+#pragma unroll
+        for (int r = 0; r < 16; r++) ld_pair<T>(ld, o, col, j + 16 * r, v[r].x, v[r].y);
+        butterfly<16, false>(v);  // first stage: no twiddles
+        T2* y = buf + p * PL;
+#pragma unroll
+        for (int r = 0; r < 16; r++) y[pad16(16 * j + r)] = v[r];
+        __syncthreads();
+        {
+            T2* z = buf + pp * PL;
+#pragma unroll
+            for (int r = 0; r < 16; r++) v[r] = z[pad16(jp + 16 * r)];
+            stage2_16x16<false>(v, tw, jp);
+#pragma unroll
+            for (int r = 0; r < 16; r++) z[pad16(jp + 16 * r)] = v[r];
+        }
+        __syncthreads();
+        // unpack: modes k and n-k of both columns of pair p from Z[k], Z[n-k]
+        const T2* z = buf + pl_ * PL;
+        const int col2 = c0 + 2 * pl_;
+#pragma unroll
+        for (int u = 0; u < H / 16; u++) {
+            const int k = jl + 16 * u;
+            if (k == 0) {
+                const T2 a = z[pad16(0)], b = z[pad16(H)];
+                st_pair<T>(st, o, col2, 0, a.x * sc, a.y * sc);
+                st_pair<T>(st, o, col2, H, b.x * sc, b.y * sc);
+            } else {
+                const T2 a = z[pad16(k)], b = z[pad16(N - k)];
+                st_pair<T>(st, o, col2, k, T(0.5) * (a.x + b.x) * sc, T(0.5) * (a.y + b.y) * sc);
+                st_pair<T>(st, o, col2, N - k, T(0.5) * (a.y - b.y) * sc, T(0.5) * (b.x - a.x) * sc);
+            }
+        }
+    } else {
+        // pack: points k and n-k of pair p (k = 0 takes 0 and n/2) into Z
+        {
+            constexpr int U = H / 16;
+            const int col = c0 + 2 * pl_;
+            T a1[U], b1[U], a2[U], b2[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int k = jl + 16 * u;
+                ld_pair<T>(ld, o, col, k, a1[u], b1[u]);
+                ld_pair<T>(ld, o, col, k == 0 ? H : N - k, a2[u], b2[u]);
+            }
+            T2* z = buf + pl_ * PL;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int k = jl + 16 * u;
+                T2 lo, hi;
+                if (k == 0) {
+                    lo.x = a1[u]; lo.y = b1[u];
+                    hi.x = a2[u]; hi.y = b2[u];
+                    z[pad16(0)] = lo;
+                    z[pad16(H)] = hi;
+                } else {
+                    lo.x = a1[u] - b2[u]; lo.y = a2[u] + b1[u];
+                    hi.x = a1[u] + b2[u]; hi.y = b1[u] - a2[u];
+                    z[pad16(k)] = lo;
+                    z[pad16(N - k)] = hi;
+                }
+            }
+        }
+        __syncthreads();
+        T2 v[16];
+        {
+            // first stage: slots j + 16 r in, 16 j + r out (all reads before any write)
+            T2* z = buf + pp * PL;
+#pragma unroll
+            for (int r = 0; r < 16; r++) v[r] = z[pad16(jp + 16 * r)];
+            butterfly<16, true>(v);
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 16; r++) z[pad16(16 * jp + r)] = v[r];
+        }
+        __syncthreads();
+        const int p = STORE_CF ? pl_ : pp, k = STORE_CF ? jl : jp, col = c0 + 2 * p;
+        const T2* z = buf + p * PL;
+#pragma unroll
+        for (int r = 0; r < 16; r++) v[r] = z[pad16(k + 16 * r)];
+        stage2_16x16<true>(v, tw, k);
+#pragma unroll
+        for (int r = 0; r < 16; r++) st_pair<T>(st, o, col, k + 16 * r, v[r].x * sc, v[r].y * sc);
+    }
+}
+
 }  // namespace sw

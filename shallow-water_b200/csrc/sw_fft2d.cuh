@@ -130,6 +130,21 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
     // compile-time pair kernels for the common lengths when the tile matches and
     // every tile is full (the generic kernel covers the rest)
     constexpr bool pair_ok = INV ? LCF : SCF;
+    if constexpr (pair_ok && sizeof(T) == 4) {
+        if (plan.n == FFT_R_N && tc == 2 * FFT_R_NP && ncols % tc == 0) {
+            auto kern = k_fft_pass_r<T, INV, LCF, SCF, LD, ST>;
+            static int attr_r[64] = {};
+            if (dev < 64 && !attr_r[dev]) {
+                SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+                attr_r[dev] = 1;
+            }
+            dim3 grid(ncols / tc, nout);
+            kern<<<grid, FFT_THREADS, fft_pass_smem_r<T>(), s>>>(tw, sc, ld, st);
+            SW_CHECK_LAUNCH();
+            count_launch();
+            return;
+        }
+    }
     if constexpr (pair_ok) {
         const bool s256 = plan.n == 256 && tc == (1 << LT256), s128 = plan.n == 128 && tc == (1 << LT128);
         if ((s256 || s128) && ncols % tc == 0) {

@@ -1874,16 +1874,26 @@ struct Solver {
         return ex;
     }
 
-    // nsteps steps as graph launches; one synchronisation at the end, where the
-    // sticky status of the pressure solves is checked.
-    int advance_graph(int nsteps, bool ggen_first) {
-        long long fixed = 0;
+    // nsteps steps as graph launches queued on the context's stream (no host
+    // synchronisation); advance_finish() waits for them and checks the sticky
+    // status of the pressure solves.
+    void advance_enqueue(int nsteps, bool ggen_first) {
         for (int k = 0; k < nsteps; k++) {
             const bool g = k == 0 ? ggen_first : true;
             SW_CUDA(cudaGraphLaunch(step_graph(g), st));
-            fixed += k_fixed[g ? 1 : 0];
+            pending_fixed += k_fixed[g ? 1 : 0];
             t += 1.0 / (double)ng;
         }
+        pending = true;
+    }
+    int advance_graph(int nsteps, bool ggen_first) {
+        advance_enqueue(nsteps, ggen_first);
+        return advance_finish();
+    }
+    int advance_finish() {
+        const long long fixed = pending_fixed;
+        pending_fixed = 0;
+        pending = false;
         int* h = reinterpret_cast<int*>(h_pinned);
         long long* hx = reinterpret_cast<long long*>(h_pinned + 4);
         SW_CUDA(cudaMemcpyAsync(h, err_dev.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1910,6 +1920,8 @@ struct Solver {
         return SW_OK;
     }
     bool use_graphs = true;
+    bool pending = false;        // steps queued by advance_enqueue and not yet finished
+    long long pending_fixed = 0; // their kernel launches outside the sweep loops
     bool fused_prepare = true;  // psolve set-up as eight fused batched transforms
     bool last_from_graph = false;
 };

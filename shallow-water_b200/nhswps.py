@@ -155,6 +155,17 @@ def advance(state, output=None, nsteps=1):
     return state
 
 
+def advance_async(spectral, nsteps=1, ggen=True):
+    """Queue nsteps graph-captured steps of every member of the context without
+    waiting (see sync); contexts on different streams run concurrently."""
+    check(lib().sw_advance_async(spectral.ctx, int(nsteps), int(bool(ggen))))
+
+
+def sync(spectral):
+    """Wait for the context's queued work; raises if a pressure solve failed."""
+    check(lib().sw_sync(spectral.ctx))
+
+
 def last_sweeps(spectral):
     out = (ctypes.c_int * 3)()
     check(lib().sw_last_sweeps(spectral.ctx, out))
