@@ -218,6 +218,11 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     M = args.members
     sp = sw.Spectral(NG, NZ, precision=prec, nmembers=M, device=local)
     sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
+    fft_pre = None
+    if full:  # the top kernel's pass (102 planes, one launch), timed on this context's stream
+        chunk = sp.set_fft_chunk(0)
+        fft_pre = time_fft_pass(sw, sp, 6 * (NZ + 1), w_fft)
+        sp.set_fft_chunk(chunk)
     tune = sp.autotune() if args.autotune == "on" else None
     qq2 = sw.vstrip.pv_strip(NG)
     for m in range(M):
@@ -284,7 +289,8 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
                       "h2d_bytes_per_step": 4 * n3 * 8, "d2h_bytes_per_step": 3 * n3 * 8, "steps": e2e_steps}
         planes = 6 * (NZ + 1)
         per_launch_s, bytes_per_launch = time_fft_pass(sw, sp, planes, w_fft)
-        res["fft"] = {"planes": planes, "per_launch_s": per_launch_s, "bytes": bytes_per_launch}
+        res["fft"] = {"planes": planes, "per_launch_s": fft_pre[0], "bytes": fft_pre[1],
+                      "per_launch_s_after_run": per_launch_s}
     sp.close()
     torch.cuda.synchronize()
     return res

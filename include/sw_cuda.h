@@ -119,8 +119,8 @@ int sw_advance(sw_ctx* ctx, int nsteps, int ggen);
  * the host with one synchronisation per sweep (enable = 0).  Same results. */
 int sw_set_graphs(sw_ctx* ctx, int enable);
 /* Tuning of the batched 2-D transforms: planes per pair of tile-pass launches
- * (1 .. the context's capacity, 6*(nz+1)*nmembers).  *in_use (may be NULL) gets
- * the clamped value.  Results do not depend on it.  No reference counterpart:
+ * (1 .. the context's capacity, 6*(nz+1)*nmembers; planes <= 0 only queries).
+ * *in_use (may be NULL) gets the value now in use.  Results do not depend on it.  No reference counterpart:
  * the reference transforms one plane at a time (src/sta2dfft.rs:91-123). */
 int sw_set_fft_chunk(sw_ctx* ctx, int planes, int* in_use);
 /* Autotuner of that chunk: times reps forward + inverse transforms of the

@@ -545,8 +545,8 @@ k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
 }
 
 // ---------------------------------------------------------------------------
-// Register-staged pass for n = 256 = 16 x 16 with 16 column pairs per tile (the
-// float32 tile): 256 threads, one radix-16 butterfly each per stage.  The
+// Register-staged pass for n = 256 = 16 x 16 with 16 column pairs (32 columns)
+// per tile: 256 threads, one radix-16 butterfly each per stage.  The
 // butterfly next to global memory runs on registers: a forward pass loads the 16
 // points j + 16 r of its pair straight into the first butterfly, and a reverse
 // pass stores the 16 modes j + 16 r of its second butterfly straight to global
@@ -563,19 +563,38 @@ inline size_t fft_pass_smem_r() {
 
 // Second radix-16 stage of 256 = 16 x 16 on the slots j + 16 r of one sequence:
 // twiddles exp(-+2 pi i r j / 256), then the butterfly; natural order in and out.
+// Four twiddles come from the table (r = 1, 2, 4, 8); the other eleven are
+// products of at most three of them, which keeps shared-memory instructions (the
+// pass's limiting pipe) down at a cost of a few roundings per twiddle.
 template <bool INV, typename T2>
 __device__ __forceinline__ void stage2_16x16(T2* v, const T2* __restrict__ tw, int j) {
+    T2 w[16];
+    w[1] = tw[j];
+    w[2] = tw[2 * j];
+    w[4] = tw[4 * j];
+    w[8] = tw[8 * j];
+    w[3] = cmul(w[1], w[2]);
+    w[5] = cmul(w[1], w[4]);
+    w[6] = cmul(w[2], w[4]);
+    w[7] = cmul(w[3], w[4]);
+    w[9] = cmul(w[1], w[8]);
+    w[10] = cmul(w[2], w[8]);
+    w[11] = cmul(w[3], w[8]);
+    w[12] = cmul(w[4], w[8]);
+    w[13] = cmul(w[5], w[8]);
+    w[14] = cmul(w[6], w[8]);
+    w[15] = cmul(w[7], w[8]);
 #pragma unroll
     for (int r = 1; r < 16; r++) {
-        T2 w = tw[r * j];
-        if (INV) w.y = -w.y;
-        v[r] = cmul(v[r], w);
+        T2 ww = w[r];
+        if (INV) ww.y = -ww.y;
+        v[r] = cmul(v[r], ww);
     }
     butterfly<16, INV>(v);
 }
 
 template <typename T, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
-__global__ void __launch_bounds__(FFT_THREADS, 3)
+__global__ void __launch_bounds__(FFT_THREADS, sizeof(T) == 8 ? 2 : 4)
 k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
     using T2 = typename C2<T>::t;
     static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");

@@ -130,11 +130,12 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
     // compile-time pair kernels for the common lengths when the tile matches and
     // every tile is full (the generic kernel covers the rest)
     constexpr bool pair_ok = INV ? LCF : SCF;
-    if constexpr (pair_ok && sizeof(T) == 4) {
+    if constexpr (pair_ok) {
         if (plan.n == FFT_R_N && tc == 2 * FFT_R_NP && ncols % tc == 0) {
             auto kern = k_fft_pass_r<T, INV, LCF, SCF, LD, ST>;
             static int attr_r[64] = {};
             if (dev < 64 && !attr_r[dev]) {
+                SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
                 attr_r[dev] = 1;
             }
@@ -205,7 +206,8 @@ struct Fft2d {
         cap = cap_planes;
         mid.alloc((size_t)cap * ng * ng);
         chunk = default_chunk(ng, cap);
-        tc = pick_tile<T>(ng);
+        // n = 256: the register-staged pass with 32-column tiles (one buffer)
+        tc = ng == FFT_R_N ? 2 * FFT_R_NP : pick_tile<T>(ng);
         sc = (T)(1.0 / std::sqrt((double)ng));
     }
     // Planes per launch pair, clamped to [1, cap]; returns the value in use.

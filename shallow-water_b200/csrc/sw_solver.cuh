@@ -388,6 +388,8 @@ struct Solver {
     // Planes per 2-D transform launch pair; the captured step graphs hold the old
     // launch sequence, so they are dropped and re-captured on the next step.
     int set_fft_chunk(int planes) {
+        if (planes <= 0) return fft.chunk;  // query
+        if (planes == fft.chunk || (planes > fft.cap && fft.chunk == fft.cap)) return fft.chunk;
         SW_CUDA(cudaStreamSynchronize(st));
         for (auto& e : step_exec)
             if (e) {
@@ -1752,8 +1754,7 @@ struct Solver {
             SW_UPDATE_CASE(5)
             SW_UPDATE_CASE(9)
             SW_UPDATE_CASE(17)
-            SW_UPDATE_CASE(33)
-            default: break;
+            default: break;  // deeper columns: the streamed loop below (registers would spill)
         }
 #undef SW_UPDATE_CASE
         for_cols(st, M * n2, [=] __device__(int c) {

@@ -59,7 +59,8 @@ class Spectral:
         return self._ctx
 
     def set_fft_chunk(self, planes):
-        """Planes per pair of 2-D transform launches (clamped); returns the value in use."""
+        """Planes per pair of 2-D transform launches (clamped; <= 0 only queries);
+        returns the value in use."""
         v = ctypes.c_int()
         check(lib().sw_set_fft_chunk(self._ctx, int(planes), ctypes.byref(v)))
         return v.value
