@@ -30,6 +30,12 @@ PKG_DIR = os.path.join(ROOT, "shallow-water_b200")
 NG, NZ = 256, 16
 METRIC = "member-steps/s at ng=256 nz=16"
 UNIT = "member-steps/s"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, ncu) of one tile pass
+# over 102 planes at ng=256, averaged over the two forward and two reverse passes
+# of the transform micro-benchmark.  Reads are the plane data; the written planes
+# mostly stay in the 126 MB L2 until after the kernel, so little write traffic is
+# attributed to the pass itself.
+FFT_PASS_DRAM_BYTES = {"mixed": 26.86e6, "fp64": 60.4e6}
 
 
 def load_package():
@@ -226,7 +232,7 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     tune = sp.autotune() if args.autotune == "on" else None
     qq2 = sw.vstrip.pv_strip(NG)
     for m in range(M):
-        q3, d3, g3 = initial_fields(NG, NZ, 1 + rank * M + m, lambda ng: qq2)
+        q3, d3, g3 = initial_fields(NG, NZ, args.seed0 + rank * M + m, lambda ng: qq2)
         sw.nhswps.initial_state(sp, q3, d3, g3, member=m, invert=False)
     sw.nhswps.main_invert_all(sp)
     st = sw.State(sp, member=0)
@@ -423,6 +429,93 @@ def uneven(sw, args, rank, world, local):
     return 0
 
 
+def kernels(sw, args, rank, local):
+    """Standalone kernels on device buffers, timed with CUDA events (reps launches
+    after 3 warm-ups): forfft/revfft at n in {32, 96, 160, 256, 384, 512} over
+    17 n columns, float64 and float32, N(0,1) input (seed 2); batched tridiagonal
+    solves, 65,536 systems of 17 unknowns, diagonal U[2,4], off-diagonals
+    U[-1,1], right-hand side N(0,1) (seed 3).  Algorithmic bytes: one read and
+    one write of the batch per transform; a, b, c, d read and x written once per
+    tridiagonal solve."""
+    if rank != 0:
+        return 0
+    import torch
+    L = sw._native.lib()
+    peak, peak_kind = measured_peak()
+    reps = max(5, args.steps)
+    s = torch.cuda.Stream()
+    sp = ctypes.c_void_p(s.cuda_stream)
+    rows = []
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    rng = np.random.default_rng(2)
+    for n in (32, 96, 160, 256, 384, 512):
+        m = 17 * n
+        for prec_name, prec, dt in (("fp64", sw.SW_FP64, torch.float64), ("fp32", sw.SW_MIXED, torch.float32)):
+            x = torch.from_numpy(rng.standard_normal(m * n)).to(dt).cuda()
+            xp = ctypes.c_void_p(x.data_ptr())
+            nbytes = 2 * m * n * x.element_size()
+            for name, f in (("forfft", L.sw_forfft_dev), ("revfft", L.sw_revfft_dev)):
+                t = timed(lambda: sw._native.check(f(m, n, xp, prec, sp)))
+                rows.append({"kernel": name, "n": n, "columns": m, "precision": prec_name, "us": t * 1e6,
+                             "gbs": nbytes / t / 1e9, "frac": nbytes / t / 1e9 / peak})
+    rng = np.random.default_rng(3)
+    n, nsys = 17, 65536
+    arrs = [torch.from_numpy(v).cuda() for v in (rng.uniform(-1, 1, (n, nsys)), rng.uniform(2, 4, (n, nsys)),
+                                                  rng.uniform(-1, 1, (n, nsys)), rng.standard_normal((n, nsys)))]
+    xo = torch.empty_like(arrs[0])
+    ptrs = [ctypes.c_void_p(v.data_ptr()) for v in arrs] + [ctypes.c_void_p(xo.data_ptr())]
+    t = timed(lambda: sw._native.check(L.sw_tridiag_batched(n, nsys, *ptrs, sp)))
+    nbytes = 5 * n * nsys * 8
+    rows.append({"kernel": "tridiag_batched", "n": n, "systems": nsys, "precision": "fp64", "us": t * 1e6,
+                 "gbs": nbytes / t / 1e9, "frac": nbytes / t / 1e9 / peak})
+    print(json.dumps({"mode": "kernels", "peak_gbs": peak, "peak_kind": peak_kind, "reps": reps,
+                      "note": "inputs below the 126 MB L2 for small n: the smaller cases partly run from L2",
+                      "rows": rows}), flush=True)
+    return 0
+
+
+def accuracy(sw, args, rank, local):
+    """Mixed vs FP64 on one member at (--ng, --nz) after --steps steps from the
+    same vstrip + N(0,1e-3) initial state: rel-L2 of each prognostic field and of
+    h = z(nz)/HBAR - 1, and the step rates."""
+    if rank != 0:
+        return 0
+    import torch
+    L = sw._native.lib()
+    qq2 = sw.vstrip.pv_strip(NG)
+    q3, d3, g3 = initial_fields(NG, NZ, args.seed0, lambda ng: qq2)
+    res, rates = {}, {}
+    for prec_name, prec in (("fp64", sw.SW_FP64), ("mixed", sw.SW_MIXED)):
+        sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+        st = sw.nhswps.initial_state(sp, q3, d3, g3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sw._native.check(L.sw_advance(sp.ctx, args.steps, 1))
+        rates[prec_name] = args.steps / (time.perf_counter() - t0)
+        f = {k: st.get(k).ravel(order="F") for k in ("qs", "ds", "gs", "pn", "u", "z")}
+        f["h"] = f["z"][-NG * NG:] / 0.4 - 1.0
+        res[prec_name] = f
+        sp.close()
+    err = {k: float(np.linalg.norm(res["mixed"][k] - res["fp64"][k]) / max(np.linalg.norm(res["fp64"][k]), 1e-300))
+           for k in res["fp64"]}
+    print(json.dumps({"mode": "accuracy", "ng": NG, "nz": NZ, "steps": args.steps,
+                      "workload": "one member, vstrip + N(0,1e-3) q, delta=gamma=0",
+                      "mixed_rel_l2_vs_fp64": err, "steps_per_s_incl_first_graph_capture": rates}), flush=True)
+    return 0
+
+
 def main():
     global NG, NZ, METRIC
     ap = argparse.ArgumentParser()
@@ -442,6 +535,13 @@ def main():
     ap.add_argument("--planes", type=int, default=None, help="planes of the --fft-only pass (default 6*(nz+1))")
     ap.add_argument("--ng", type=int, default=NG, help="horizontal grid (the headline workload is 256)")
     ap.add_argument("--nz", type=int, default=NZ, help="layers (the headline workload is 16)")
+    ap.add_argument("--kernels", action="store_true",
+                    help="time the standalone kernels: forfft/revfft at n in {32,...,512} (17n columns, FP64 and "
+                         "FP32) and the batched tridiagonal solve (65,536 x 17)")
+    ap.add_argument("--seed0", type=int, default=1, help="seed of member 0 (member m uses seed0 + m)")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="run one member --steps steps in FP64 and in the mixed path at (--ng, --nz) and report "
+                         "their rel-L2 differences (the ng=512 nz=32 sweep)")
     ap.add_argument("--drift", type=int, default=0, metavar="STEPS",
                     help="instead of timing: run one member STEPS steps in FP64 and in the mixed path and "
                          "report energy and PV drift")
@@ -475,6 +575,10 @@ def main():
         prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
         sp = sw.Spectral(NG, NZ, precision=prec, nmembers=1, device=local)
         return fft_only(sw, sp, args, 8 if prec == sw.SW_FP64 else 4)
+    if args.kernels:
+        return kernels(sw, args, rank, local)
+    if args.accuracy:
+        return accuracy(sw, args, rank, local)
     if args.drift:
         return drift(sw, args, rank, local)
     if args.uneven:
@@ -489,11 +593,7 @@ def main():
     w_fft = main_arm["w_fft"]
     peak, peak_kind = measured_peak()
     achieved = main_arm["fft"]["bytes"] / main_arm["fft"]["per_launch_s"] / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "fft_pass_traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            traffic = json.load(f).get("bytes_per_launch_%s" % args.precision)
+    traffic = FFT_PASS_DRAM_BYTES.get(args.precision) if (NG, NZ) == (256, 16) else None
     step_bytes = algorithmic_bytes_per_step(NG, NZ, main_arm["sweeps"], w_fft)
     step_gbs = step_bytes * (args.steps * M / main_arm["t_local"]) / 1e9
 

@@ -155,6 +155,16 @@ int sw_sync(sw_ctx* ctx);
 /* Device pointer of a state field (all members, member-major) and its element size
  * in bytes (8 for the float64 fields; 4 for float32 fields of SW_MIXED). */
 int sw_field_device_ptr(sw_ctx* ctx, int field, void** ptr, int* elem_bytes);
+/* Batched tridiagonal solves, float64: nsys independent systems of n <= 33
+ * unknowns, a[i] x[i-1] + b[i] x[i] + c[i] x[i+1] = d[i] (a[0], c[n-1] unused),
+ * level-major with the system index contiguous ([s + nsys*i]); no pivoting.  The
+ * vertical Thomas solve of psolve (src/nhswps/psolve.rs:285-327) for general
+ * coefficients; the reference has no standalone entry point.  Device arrays on
+ * `stream`; the _host variant copies host arrays through device memory. */
+int sw_tridiag_batched(int n, int nsys, const double* a, const double* b, const double* c, const double* d,
+                       double* x, void* stream);
+int sw_tridiag_batched_host(int n, int nsys, const double* a, const double* b, const double* c, const double* d,
+                            double* x);
 /* The context's CUDA stream (cudaStream_t as void*). */
 int sw_stream(sw_ctx* ctx, void** stream);
 /* Batched 2-D transforms on device memory with the context's plan: direction 0 =

@@ -9,8 +9,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libswcuda.so")
-SOURCES = ["sw_capi.cu", "sw_noalloc.cu"]
-DEPS = ["sw_capi.cu", "sw_noalloc.cu", "sw_solver.cuh", "sw_fft2d.cuh", "sw_fft.cuh", "sw_core.cuh", "sw_spectral_host.h"]
+SOURCES = ["sw_capi.cu", "sw_noalloc.cu", "sw_tridiag.cu"]
+DEPS = ["sw_capi.cu", "sw_noalloc.cu", "sw_tridiag.cu", "sw_solver.cuh", "sw_fft2d.cuh", "sw_fft.cuh", "sw_core.cuh", "sw_spectral_host.h"]
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo", "--extended-lambda",
     "-gencode", "arch=compute_100a,code=sm_100a",

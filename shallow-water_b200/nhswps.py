@@ -110,6 +110,21 @@ def psolve(state, nitmax=100):
     return it.value, e.value
 
 
+def tridiag_batched(a, b, c, d):
+    """Solve nsys tridiagonal systems of n <= 33 unknowns in float64 on the GPU
+    (the vertical Thomas solve of psolve.rs:285-327 for general coefficients).
+    Arrays have shape (n, nsys), system index contiguous:
+    a[i] x[i-1] + b[i] x[i] + c[i] x[i+1] = d[i].  Returns x, shape (n, nsys)."""
+    arrs = [np.ascontiguousarray(np.asarray(v, dtype=np.float64)) for v in (a, b, c, d)]
+    n, nsys = arrs[0].shape
+    for v in arrs:
+        if v.shape != (n, nsys):
+            raise ValueError("a, b, c, d need the same (n, nsys) shape")
+    x = np.zeros((n, nsys))
+    check(lib().sw_tridiag_batched_host(n, nsys, *[dptr(v) for v in arrs], dptr(x)))
+    return x
+
+
 def source(state, sqs=None, sds=None, sgs=None):
     """Nonlinear source terms in spectral space (src/nhswps/source.rs:19-138)."""
     n = _n3(state)
