@@ -28,6 +28,56 @@ inline void upload(DevBuf<double>& d, const std::vector<double>& h) {
     SW_CUDA(cudaMemcpy(d.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
 }
 
+// Second pass of the pressure sweep's p, p_x, p_y transforms: output o of a chunk
+// is (member mm, kind, level iz), o = (mm * 3 + kind) * nz + iz; kinds 0 and 2 read
+// the intermediates of p and p_y, kind 1 reads p's with kx mirrored and the d/dx
+// factor (src/sta2dfft.rs:128-155).  Columns (iy) are contiguous on both sides.
+template <typename T>
+struct SweepMidLoad {
+    using T2 = typename C2<T>::t;
+    static constexpr bool pair_io = true;
+    const T* mid;
+    int ng, nz;
+    __device__ __forceinline__ const T* row(int o, int kx, double& f) const {
+        const int mm = o / (3 * nz), k = o - mm * 3 * nz, kind = k / nz, iz = k - kind * nz;
+        const int plane = mm * 2 * nz + (kind == 2 ? nz : 0) + iz;
+        f = kind == 1 ? dmul(kx, ng) : 1.0;
+        return mid + ((size_t)plane * ng + (kind == 1 ? mirror(kx, ng) : kx)) * ng;
+    }
+    __device__ __forceinline__ T operator()(int o, int c, int p) const {
+        double f;
+        const T* rw = row(o, p, f);
+        return (T)(f * (double)rw[c]);
+    }
+    __device__ __forceinline__ T2 ld2(int o, int c, int p) const {
+        double f;
+        const T* rw = row(o, p, f);
+        T2 v = *reinterpret_cast<const T2*>(rw + c);
+        v.x = (T)(f * (double)v.x);
+        v.y = (T)(f * (double)v.y);
+        return v;
+    }
+};
+template <typename T>
+struct SweepPhysStore {
+    using T2 = typename C2<T>::t;
+    static constexpr bool pair_io = true;
+    T *A, *B, *C;
+    int ng, nz, L, m0;
+    __device__ __forceinline__ T* dst(int o, int c, int p) const {
+        const int mm = o / (3 * nz), k = o - mm * 3 * nz, kind = k / nz, iz = k - kind * nz;
+        T* base = kind == 0 ? A : kind == 1 ? B : C;
+        return base + ((size_t)((m0 + mm) * L + iz) * ng + p) * ng + c;
+    }
+    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { *dst(o, c, p) = v; }
+    __device__ __forceinline__ void st2(int o, int c, int p, T a, T b) const {
+        T2 v;
+        v.x = a;
+        v.y = b;
+        *reinterpret_cast<T2*>(dst(o, c, p)) = v;
+    }
+};
+
 constexpr int UPDATE_THREADS = 128;
 
 // Semi-implicit update of one (kx, ky) column (advance.rs:60-279; the same
@@ -496,6 +546,7 @@ struct Solver {
             wkh[c] = s * rope[i];
         });
         T *R = r, *U = u, *V = v, *ZE = zeta;
+        T *SU = W(8), *SV = W(9);  // spectral u, v for psolve's set-up in this stage
         fft.spctop(st, 4 * ML,
             [=] __device__(int o, int kx, int ky) -> T {
                 const int which = o / ML, q = o - which * ML, m = q / L;
@@ -509,9 +560,14 @@ struct Solver {
                 if (which == 0) return (T)wka(i);
                 if (which == 1) return (T)wkb(i);
                 const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
-                if (which == 2)
-                    return (T)(dmul(kx, ng) * (rlap[mx] * dsq[mx]) - dmul(ky, ng) * (rlap[my] * wkb(my)));
-                return (T)(dmul(ky, ng) * (rlap[my] * dsq[my]) + dmul(kx, ng) * (rlap[mx] * wkb(mx)));
+                if (which == 2) {
+                    const T val = (T)(dmul(kx, ng) * (rlap[mx] * dsq[mx]) - dmul(ky, ng) * (rlap[my] * wkb(my)));
+                    SU[(size_t)q * n2 + i] = val;
+                    return val;
+                }
+                const T val = (T)(dmul(ky, ng) * (rlap[my] * dsq[my]) + dmul(kx, ng) * (rlap[mx] * wkb(mx)));
+                SV[(size_t)q * n2 + i] = val;
+                return val;
             },
             [=] __device__(int o, int iy, int ix, T val) {
                 const int which = o / ML, q = o - which * ML;
@@ -1038,8 +1094,13 @@ struct Solver {
         }
         // P1: forward transforms of everything physical that is known now (z only on
         // the float64 path; the float32 path filled S1 above)
-        const int o_z = ML, o_a = ML + (mixed ? 0 : Mnz), o_b = o_a + ML, o_p = o_b + ML, o_u = o_p + ML,
-                  o_v = o_u + ML, o_h = o_v + ML;
+        // Inside advance (hints set by the step), main_invert of this stage has just
+        // written the spectra of u and v to Su, Sv, and the previous pressure solve
+        // of this step left its solution in ps (= ptospc(pn)), so those forward
+        // transforms are skipped.
+        const bool uv_ready = hint_uv_spec, ps_ready = hint_ps_guess;
+        const int o_z = ML, o_a = ML + (mixed ? 0 : Mnz), o_b = o_a + ML, o_p = o_b + ML,
+                  o_u = o_p + (ps_ready ? 0 : ML), o_v = o_u + (uv_ready ? 0 : ML), o_h = o_v + (uv_ready ? 0 : ML);
         const int n1 = o_h + (mixed ? 0 : M);
         fft.ptospc(st, n1,
             [=] __device__(int o, int iy, int ix) -> T {
@@ -1334,19 +1395,24 @@ struct Solver {
         //     theta derivatives of the reference (psolve.rs:96-240) are linear in p,
         //     so they are formed from these in physical space in (b): 3 nz transforms
         //     per member instead of the 4 nz - 1 of the derived quantities.
-        const int n3z = 3 * nz;
-        fft.spctop(st, M * n3z,
-            [=] __device__(int o, int kx, int ky) -> T {
-                const int m = o / n3z, k = o - m * n3z, kind = k / nz, iz = k - kind * nz;
-                const double* pc = PS + (size_t)(m * L + iz) * n2;
-                if (kind == 0) return (T)pc[kx + ng * ky];
-                if (kind == 1) return (T)(dmul(kx, ng) * pc[mirror(kx, ng) + ng * ky]);
-                return (T)(dmul(ky, ng) * pc[kx + ng * mirror(ky, ng)]);
-            },
-            [=] __device__(int o, int iy, int ix, T val) {
-                const int m = o / n3z, k = o - m * n3z, kind = k / nz, iz = k - kind * nz;
-                (kind == 0 ? A : kind == 1 ? B : C)[(size_t)(m * L + iz) * n2 + iy + ng * ix] = val;
-            });
+        //     d/dx acts on kx, which the first (reverse, along ky) pass leaves alone, so
+        //     p_x takes p's intermediate with the derivative applied in the second
+        //     pass: 2 nz first passes and 3 nz second passes per member.
+        const int n2z = 2 * nz;
+        const int mchunk = std::max(1, std::min(M, fft.chunk / n2z));
+        for (int m0 = 0; m0 < M; m0 += mchunk) {
+            const int mc = std::min(mchunk, M - m0);
+            launch_pass<T, true, true, false>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, n2z * mc, ng,
+                [=] __device__(int o, int kx, int ky) -> T {
+                    const int mm = o / n2z, k = o - mm * n2z, kind = k / nz, iz = k - kind * nz;
+                    const double* pc = PS + (size_t)((m0 + mm) * L + iz) * n2;
+                    if (kind == 0) return (T)pc[kx + ng * ky];
+                    return (T)(dmul(ky, ng) * pc[kx + ng * mirror(ky, ng)]);
+                },
+                MidPC<T>{fft.mid.p, ng});
+            launch_pass<T, true, true, true>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, 3 * nz * mc, ng,
+                SweepMidLoad<T>{fft.mid.p, ng, nz}, SweepPhysStore<T>{A, B, C, ng, nz, L, m0});
+        }
         // (b) total source S = S0 + S1(p), to spectral space
         fft.ptospc(st, ML,
             [=] __device__(int q, int iy, int ix) -> T {
@@ -1582,8 +1648,13 @@ struct Solver {
                 if (which == 0) F[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
                 else (which == 1 ? Su : Sv)[(size_t)q * n2 + i] = val;
             });
-        // q, delta, ff, ffx, ffy, (ux, uy, vx, vy), z(0) derivatives to physical space
-        const int nf2 = (5 + 2 * nuv) * ML;
+        // q, delta, ff, ffx, ffy, (ux, uy, vx, vy), z(0) derivatives to physical space.
+        // When this stage's main_invert has run, q = zeta - f r pointwise (main_invert
+        // sets zeta = spctop(qs + f rhat), r = spctop(rhat)), so q is not transformed.
+        const bool q_phys = hint_q_phys;
+        const int q0 = q_phys ? 1 : 0;  // first transformed field
+        T *ZE = zeta, *R = r;
+        const int nf2 = (5 - q0 + 2 * nuv) * ML;
         fft.spctop(st, nf2 + 2 * M,
             [=] __device__(int o, int kx, int ky) -> T {
                 const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
@@ -1592,7 +1663,7 @@ struct Solver {
                     const T* s = zs0 + (size_t)m * n2;
                     return which == 0 ? (T)(dmul(kx, ng) * (double)s[mx]) : (T)(dmul(ky, ng) * (double)s[my]);
                 }
-                const int which = o / ML, q = o - which * ML;
+                const int which = o / ML + q0, q = o - (which - q0) * ML;
                 if (which < 2) return (T)(which == 0 ? QS : DS)[(size_t)q * n2 + kx + ng * ky];
                 const int w2 = which - 2;  // 0..2: F, F_x, F_y; 3..6: u_x, u_y, v_x, v_y
                 const T* s = (w2 < 3 ? F : w2 < 5 ? Su : Sv) + (size_t)q * n2;
@@ -1608,7 +1679,7 @@ struct Solver {
                     (which == 0 ? zx0 : zy0)[(size_t)m * n2 + i] = val;
                     return;
                 }
-                const int which = o / ML, q = o - which * ML;
+                const int which = o / ML + q0, q = o - (which - q0) * ML;
                 T* out = which == 0 ? Q : which == 1 ? DD : which == 2 ? FF : which == 3 ? FX : which == 4 ? FY
                        : which == 5 ? UX : which == 6 ? UY : which == 7 ? VX : VY;
                 out[(size_t)q * n2 + i] = val;
@@ -1620,8 +1691,11 @@ struct Solver {
                 const int i = iy + ng * ix;
                 const size_t p = (size_t)q * n2 + i;
                 switch (which) {
-                    case 0: return Q[p] * U[p];
-                    case 1: return Q[p] * V[p];
+                    case 0:
+                    case 1: {
+                        const T qv = q_phys ? (T)((double)ZE[p] - COF * (double)R[p]) : Q[p];
+                        return qv * (which == 0 ? U[p] : V[p]);
+                    }
                     case 2: {
                         const T bx = iz == 0 ? zx0[(size_t)m * n2 + i] : ZX[p];
                         const T by = iz == 0 ? zy0[(size_t)m * n2 + i] : ZY[p];
@@ -1808,20 +1882,25 @@ struct Solver {
         int it = 0;
         double e = 0.0;
         last_sweeps[0] = last_sweeps[1] = last_sweeps[2] = 0;
+        StepHints hints(*this);
         if (ggen) {
             main_invert();
+            hints.before_psolve(false);
             int stt = psolve(100, &it, &e);
             last_sweeps[0] = it;
             if (stt) return stt;
         }
         diagnose_record();
+        hints.before_source(ggen);
         source(WD(4), WD(5), WD(7), ggen && fused_prepare);
         advance_update(true);
         for (int k = 0; k < 2; k++) {
             main_invert();
+            hints.before_psolve(ggen || k > 0);
             int stt = psolve(100, &it, &e);
             last_sweeps[1 + k] = it;
             if (stt) return stt;
+            hints.before_source(true);
             source(WD(4), WD(5), WD(7), fused_prepare);
             advance_update(false);
         }
@@ -1830,21 +1909,44 @@ struct Solver {
         return SW_OK;
     }
 
+    // Sets the reuse hints for the calls of one step and clears them when the step
+    // ends (also on an error), so that the per-function entry points never see them.
+    struct StepHints {
+        Solver& s;
+        explicit StepHints(Solver& sv) : s(sv) {}
+        ~StepHints() { s.hint_uv_spec = s.hint_ps_guess = s.hint_q_phys = false; }
+        // main_invert of this stage ran; a psolve of this step already finished?
+        void before_psolve(bool previous_solve_this_step) {
+            s.hint_uv_spec = s.fused_prepare;
+            s.hint_ps_guess = s.fused_prepare && previous_solve_this_step;
+            s.hint_q_phys = false;
+        }
+        void before_source(bool invert_this_stage) {
+            s.hint_uv_spec = s.hint_ps_guess = false;
+            s.hint_q_phys = invert_this_stage;
+        }
+    };
+
     // The work of one step as captured into a CUDA graph: the three pressure
     // solves iterate inside conditional WHILE nodes, so a step needs no host
     // round trip.
     void advance_captured(bool ggen) {
         SW_CUDA(cudaMemsetAsync(sweeps_dev.p, 0, sizeof(int) * 3 * M, st));
+        StepHints hints(*this);
         if (ggen) {
             main_invert();
+            hints.before_psolve(false);
             psolve_captured(100, 0);
         }
         diagnose_record();
+        hints.before_source(ggen);
         source(WD(4), WD(5), WD(7), ggen && fused_prepare);
         advance_update(true);
         for (int k = 0; k < 2; k++) {
             main_invert();
+            hints.before_psolve(ggen || k > 0);
             psolve_captured(100, 1 + k);
+            hints.before_source(true);
             source(WD(4), WD(5), WD(7), fused_prepare);
             advance_update(false);
         }
@@ -1921,6 +2023,11 @@ struct Solver {
         return SW_OK;
     }
     bool use_graphs = true;
+    // Set by the advance flows around the calls they apply to (see
+    // psolve_prepare_fused and source): what earlier work of the same step left.
+    bool hint_uv_spec = false;  // Su, Sv hold the spectra of u, v (main_invert ran this stage)
+    bool hint_ps_guess = false; // ps holds the previous solution of this step
+    bool hint_q_phys = false;   // zeta and r are this stage's main_invert output
     bool pending = false;        // steps queued by advance_enqueue and not yet finished
     long long pending_fixed = 0; // their kernel launches outside the sweep loops
     bool fused_prepare = true;  // psolve set-up as eight fused batched transforms
