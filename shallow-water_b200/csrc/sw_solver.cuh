@@ -547,9 +547,11 @@ struct Solver {
         });
         T *R = r, *U = u, *V = v, *ZE = zeta;
         T *SU = W(8), *SV = W(9);  // spectral u, v for psolve's set-up in this stage
+        // level-major: r, zeta, u, v of one level are adjacent planes, so qs, ds, gs
+        // are read from DRAM once and from L2 by the other three
         fft.spctop(st, 4 * ML,
             [=] __device__(int o, int kx, int ky) -> T {
-                const int which = o / ML, q = o - which * ML, m = q / L;
+                const int which = o & 3, q = o >> 2, m = q / L;
                 const double* qsq = QS + (size_t)q * n2;
                 const double* dsq = DS + (size_t)q * n2;
                 const double* gsq = GS + (size_t)q * n2;
@@ -570,7 +572,7 @@ struct Solver {
                 return val;
             },
             [=] __device__(int o, int iy, int ix, T val) {
-                const int which = o / ML, q = o - which * ML;
+                const int which = o & 3, q = o >> 2;
                 T* out = which == 0 ? R : which == 1 ? ZE : which == 2 ? U : V;
                 out[(size_t)q * n2 + iy + ng * ix] = val;
             });
@@ -1098,20 +1100,24 @@ struct Solver {
         // written the spectra of u and v to Su, Sv, and the previous pressure solve
         // of this step left its solution in ps (= ptospc(pn)), so those forward
         // transforms are skipped.
+        // The first 3 ML planes are 1/(1+r), u r, v r level-major (adjacent planes
+        // share r, u, v through L2).
         const bool uv_ready = hint_uv_spec, ps_ready = hint_ps_guess;
-        const int o_z = ML, o_a = ML + (mixed ? 0 : Mnz), o_b = o_a + ML, o_p = o_b + ML,
-                  o_u = o_p + (ps_ready ? 0 : ML), o_v = o_u + (uv_ready ? 0 : ML), o_h = o_v + (uv_ready ? 0 : ML);
+        const int o_z = 3 * ML, o_p = o_z + (mixed ? 0 : Mnz);
+        const int o_u = o_p + (ps_ready ? 0 : ML), o_v = o_u + (uv_ready ? 0 : ML), o_h = o_v + (uv_ready ? 0 : ML);
         const int n1 = o_h + (mixed ? 0 : M);
         fft.ptospc(st, n1,
             [=] __device__(int o, int iy, int ix) -> T {
                 const int pi = iy + ng * ix;
-                if (o < o_z) return T(1) / (R[(size_t)o * n2 + pi] + T(1));
-                if (o < o_a) {
+                if (o < o_z) {
+                    const int q = o / 3, which = o - 3 * q;
+                    const size_t p = (size_t)q * n2 + pi;
+                    return which == 0 ? T(1) / (R[p] + T(1)) : (which == 1 ? U[p] : V[p]) * R[p];
+                }
+                if (o < o_p) {
                     const int k = o - o_z, m = k / nz, iz = 1 + k % nz;
                     return Z[(size_t)(m * L + iz) * n2 + pi];
                 }
-                if (o < o_b) { const size_t p = (size_t)(o - o_a) * n2 + pi; return U[p] * R[p]; }
-                if (o < o_p) { const size_t p = (size_t)(o - o_b) * n2 + pi; return V[p] * R[p]; }
                 if (o < o_u) return PN[(size_t)(o - o_p) * n2 + pi];
                 if (o < o_v) return U[(size_t)(o - o_u) * n2 + pi];
                 if (o < o_h) return V[(size_t)(o - o_v) * n2 + pi];
@@ -1119,14 +1125,18 @@ struct Solver {
             },
             [=] __device__(int o, int kx, int ky, T val) {
                 const int i = kx + ng * ky;
-                if (o < o_z) { Sr[(size_t)o * n2 + i] = (T)(filt[i] * (double)val); return; }
-                if (o < o_a) {
+                if (o < o_z) {
+                    const int q = o / 3, which = o - 3 * q;
+                    const size_t p = (size_t)q * n2 + i;
+                    if (which == 0) Sr[p] = (T)(filt[i] * (double)val);
+                    else (which == 1 ? SA : SB)[p] = val;
+                    return;
+                }
+                if (o < o_p) {
                     const int k = o - o_z, m = k / nz, iz = 1 + k % nz;
                     S1[(size_t)(m * L + iz) * n2 + i] = val;
                     return;
                 }
-                if (o < o_b) { SA[(size_t)(o - o_a) * n2 + i] = val; return; }
-                if (o < o_p) { SB[(size_t)(o - o_b) * n2 + i] = val; return; }
                 if (o < o_u) {  // first-guess ps, all levels (see psolve_prepare)
                     PS[(size_t)(o - o_p) * n2 + i] = (double)val;
                     return;
@@ -1263,9 +1273,11 @@ struct Solver {
                 D[(size_t)(m * L + iz) * n2 + pi] = val;
             });
         // P6: cpt2's argument and cpsource's dealiased products
+        // (level-major: the four outputs of one level are adjacent planes, so the
+        // fields they share are read from L2)
         fft.ptospc(st, 4 * ML,
             [=] __device__(int o, int iy, int ix) -> T {
-                const int which = o / ML, q = o - which * ML, m = q / L, iz = q % L;
+                const int which = o & 3, q = o >> 2, m = q / L, iz = q % L;
                 const int pi = iy + ng * ix;
                 const size_t p = (size_t)q * n2 + pi;
                 if (which == 0) return T(1) - RI[p] * RI[p] - SIGX[p] * SIGX[p] - SIGY[p] * SIGY[p];
@@ -1280,7 +1292,7 @@ struct Solver {
                 return (T)(ut * (double)VX[p] - (double)UX[p] * vt);
             },
             [=] __device__(int o, int kx, int ky, T val) {
-                const int which = o / ML, q = o - which * ML, i = kx + ng * ky;
+                const int which = o & 3, q = o >> 2, i = kx + ng * ky;
                 T* out = which == 0 ? Sc : which == 1 ? Spp : which == 2 ? Spq : Spr;
                 out[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
             });
@@ -1654,7 +1666,8 @@ struct Solver {
         const bool q_phys = hint_q_phys;
         const int q0 = q_phys ? 1 : 0;  // first transformed field
         T *ZE = zeta, *R = r;
-        const int nf2 = (5 - q0 + 2 * nuv) * ML;
+        const int nk = 5 - q0 + 2 * nuv;  // kinds per level, level-major
+        const int nf2 = nk * ML;
         fft.spctop(st, nf2 + 2 * M,
             [=] __device__(int o, int kx, int ky) -> T {
                 const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
@@ -1663,7 +1676,7 @@ struct Solver {
                     const T* s = zs0 + (size_t)m * n2;
                     return which == 0 ? (T)(dmul(kx, ng) * (double)s[mx]) : (T)(dmul(ky, ng) * (double)s[my]);
                 }
-                const int which = o / ML + q0, q = o - (which - q0) * ML;
+                const int q = o / nk, which = o - nk * q + q0;
                 if (which < 2) return (T)(which == 0 ? QS : DS)[(size_t)q * n2 + kx + ng * ky];
                 const int w2 = which - 2;  // 0..2: F, F_x, F_y; 3..6: u_x, u_y, v_x, v_y
                 const T* s = (w2 < 3 ? F : w2 < 5 ? Su : Sv) + (size_t)q * n2;
@@ -1679,15 +1692,15 @@ struct Solver {
                     (which == 0 ? zx0 : zy0)[(size_t)m * n2 + i] = val;
                     return;
                 }
-                const int which = o / ML + q0, q = o - (which - q0) * ML;
+                const int q = o / nk, which = o - nk * q + q0;
                 T* out = which == 0 ? Q : which == 1 ? DD : which == 2 ? FF : which == 3 ? FX : which == 4 ? FY
                        : which == 5 ? UX : which == 6 ? UY : which == 7 ? VX : VY;
                 out[(size_t)q * n2 + i] = val;
             });
         // products to spectral space
-        fft.ptospc(st, 6 * ML,
+        fft.ptospc(st, 6 * ML,  // level-major (outputs sharing inputs are adjacent planes)
             [=] __device__(int o, int iy, int ix) -> T {
-                const int which = o / ML, q = o - which * ML, m = q / L, iz = q % L;
+                const int q = o / 6, which = o - 6 * q, m = q / L, iz = q % L;
                 const int i = iy + ng * ix;
                 const size_t p = (size_t)q * n2 + i;
                 switch (which) {
@@ -1707,7 +1720,7 @@ struct Solver {
                 }
             },
             [=] __device__(int o, int kx, int ky, T val) {
-                const int which = o / ML, q = o - which * ML;
+                const int q = o / 6, which = o - 6 * q;
                 T* out = which == 0 ? S0 : which == 1 ? S1 : which == 2 ? S2 : which == 3 ? S3 : which == 4 ? S4 : S5;
                 out[(size_t)q * n2 + kx + ng * ky] = val;
             });
