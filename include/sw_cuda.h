@@ -74,6 +74,13 @@ int sw_state_get(sw_ctx* ctx, int field, int member, double* host, size_t n);
 /* Whole-ensemble copies: host holds nmembers*ng*ng*(nz+1) values, member-major. */
 int sw_state_set_all(sw_ctx* ctx, int field, const double* host, size_t n);
 int sw_state_get_all(sw_ctx* ctx, int field, double* host, size_t n);
+/* Same without waiting: the copies are queued on the context's stream (after any
+ * queued steps) and complete at sw_sync.  host must stay valid until then and
+ * should be page-locked for the copy to run asynchronously.  With several
+ * contexts on their own streams, one context's copies overlap another's steps.
+ * No reference counterpart. */
+int sw_state_set_all_async(sw_ctx* ctx, int field, const double* host, size_t n);
+int sw_state_get_all_async(sw_ctx* ctx, int field, double* host, size_t n);
 int sw_set_time(sw_ctx* ctx, double t);
 int sw_get_time(const sw_ctx* ctx, double* t);
 

@@ -139,7 +139,7 @@ __global__ void k_convert_back(const T* a, double* b, size_t n) {
 
 // host -> device field copy with conversion
 template <typename S>
-void field_in(S& s, int field, size_t offset, const double* host, size_t n) {
+void field_in(S& s, int field, size_t offset, const double* host, size_t n, bool sync = true) {
     if (double* d = s.field_d(field)) {
         SW_CUDA(cudaMemcpyAsync(d + offset, host, n * sizeof(double), cudaMemcpyHostToDevice, s.st));
     } else {
@@ -154,10 +154,10 @@ void field_in(S& s, int field, size_t offset, const double* host, size_t n) {
             SW_CHECK_LAUNCH();
         }
     }
-    SW_CUDA(cudaStreamSynchronize(s.st));
+    if (sync) SW_CUDA(cudaStreamSynchronize(s.st));
 }
 template <typename S>
-void field_out(S& s, int field, size_t offset, double* host, size_t n) {
+void field_out(S& s, int field, size_t offset, double* host, size_t n, bool sync = true) {
     if (double* d = s.field_d(field)) {
         SW_CUDA(cudaMemcpyAsync(host, d + offset, n * sizeof(double), cudaMemcpyDeviceToHost, s.st));
     } else {
@@ -172,7 +172,7 @@ void field_out(S& s, int field, size_t offset, double* host, size_t n) {
             SW_CUDA(cudaMemcpyAsync(host, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, s.st));
         }
     }
-    SW_CUDA(cudaStreamSynchronize(s.st));
+    if (sync) SW_CUDA(cudaStreamSynchronize(s.st));
 }
 
 // Copy nplanes host planes into a T work buffer (via float64 staging).
@@ -346,6 +346,20 @@ int sw_state_get_all(sw_ctx* ctx, int field, double* host, size_t n) {
     return with_solver(ctx, [&](auto& s) {
         require(field >= 0 && field < SW_NFIELDS && host && n == s.nf, SW_ERR_ARG, "bad field or size");
         field_out(s, field, 0, host, n);
+        return SW_OK;
+    });
+}
+int sw_state_set_all_async(sw_ctx* ctx, int field, const double* host, size_t n) {
+    return with_solver(ctx, [&](auto& s) {
+        require(field >= 0 && field < SW_NFIELDS && host && n == s.nf, SW_ERR_ARG, "bad field or size");
+        field_in(s, field, 0, host, n, false);
+        return SW_OK;
+    });
+}
+int sw_state_get_all_async(sw_ctx* ctx, int field, double* host, size_t n) {
+    return with_solver(ctx, [&](auto& s) {
+        require(field >= 0 && field < SW_NFIELDS && host && n == s.nf, SW_ERR_ARG, "bad field or size");
+        field_out(s, field, 0, host, n, false);
         return SW_OK;
     });
 }

@@ -1153,8 +1153,8 @@ struct Solver {
                 const int i = kx + ng * ky;
                 const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
                 if (o < q_x) return Sr[(size_t)o * n2 + i];
-                if (o < q_r) {
-                    const int k = o - q_x, which = k / Mnz, kk = k - which * Mnz, m = kk / nz, iz = 1 + kk % nz;
+                if (o < q_r) {  // z_x, z_y of one level adjacent
+                    const int k = o - q_x, which = k & 1, kk = k >> 1, m = kk / nz, iz = 1 + kk % nz;
                     const T* sz = S1 + (size_t)(m * L + iz) * n2;
                     return which == 0 ? (T)(dmul(kx, ng) * (double)sz[mx]) : (T)(dmul(ky, ng) * (double)sz[my]);
                 }
@@ -1167,8 +1167,8 @@ struct Solver {
                     AA[b + i] = a;
                     return (T)((double)a + DS[b + i]);
                 }
-                if (o < q_h) {
-                    const int k = o - q_d, which = k / ML, q = k - which * ML;
+                if (o < q_h) {  // u_x, u_y, v_x, v_y of one level adjacent
+                    const int k = o - q_d, which = k & 3, q = k >> 2;
                     const T* sv = (which < 2 ? Su : Sv) + (size_t)q * n2;
                     return (which & 1) == 0 ? (T)(dmul(kx, ng) * (double)sv[mx]) : (T)(dmul(ky, ng) * (double)sv[my]);
                 }
@@ -1183,13 +1183,13 @@ struct Solver {
                 const int pi = iy + ng * ix;
                 if (o < q_x) { RI[(size_t)o * n2 + pi] = val; return; }
                 if (o < q_r) {
-                    const int k = o - q_x, which = k / Mnz, kk = k - which * Mnz, m = kk / nz, iz = 1 + kk % nz;
+                    const int k = o - q_x, which = k & 1, kk = k >> 1, m = kk / nz, iz = 1 + kk % nz;
                     (which == 0 ? ZX : ZY)[(size_t)(m * L + iz) * n2 + pi] = val;
                     return;
                 }
                 if (o < q_d) { RS[(size_t)(o - q_r) * n2 + pi] = -val; return; }
                 if (o < q_h) {
-                    const int k = o - q_d, which = k / ML, q = k - which * ML;
+                    const int k = o - q_d, which = k & 3, q = k >> 2;
                     T* out = which == 0 ? UX : which == 1 ? UY : which == 2 ? VX : VY;
                     out[(size_t)q * n2 + pi] = val;
                     return;
@@ -1219,7 +1219,7 @@ struct Solver {
                     const size_t p = (size_t)(m * L + iz) * n2 + pi;
                     return which == 0 ? WW[p] : U[p] * ZX[p] + V[p] * ZY[p];
                 }
-                const int k = o - 2 * Mnz, which = k / ML, q = k - which * ML;
+                const int k = o - 2 * Mnz, which = k & 1, q = k >> 1;  // ri z_x, ri z_y of one level adjacent
                 const size_t p = (size_t)q * n2 + pi;
                 return RI[p] * (which == 0 ? ZX[p] : ZY[p]);
             },
@@ -1232,7 +1232,7 @@ struct Solver {
                     else Sd[p] = (T)(filt[i] * (double)val);
                     return;
                 }
-                const int k = o - 2 * Mnz, which = k / ML, q = k - which * ML;
+                const int k = o - 2 * Mnz, which = k & 1, q = k >> 1;
                 (which == 0 ? Sx : Sy)[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
             });
         // P5: w correction, w_x, w_y, sigx, sigy, div(sig)
@@ -1240,8 +1240,8 @@ struct Solver {
             [=] __device__(int o, int kx, int ky) -> T {
                 const int i = kx + ng * ky;
                 const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
-                if (o < 3 * Mnz) {
-                    const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
+                if (o < 3 * Mnz) {  // correction, w_x, w_y of one level adjacent
+                    const int k = o / 3, which = o - 3 * k, m = k / nz, iz = 1 + k % nz;
                     const size_t b = (size_t)(m * L + iz) * n2;
                     if (which == 0) return Sd[b + i];
                     if (which == 1) return (T)(dmul(kx, ng) * ((double)Sw[b + mx] + (double)Sd[b + mx]));
@@ -1258,7 +1258,7 @@ struct Solver {
             [=] __device__(int o, int iy, int ix, T val) {
                 const int pi = iy + ng * ix;
                 if (o < 3 * Mnz) {
-                    const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
+                    const int k = o / 3, which = o - 3 * k, m = k / nz, iz = 1 + k % nz;
                     const size_t p = (size_t)(m * L + iz) * n2 + pi;
                     if (which == 0) WW[p] = WW[p] + val;
                     else (which == 1 ? WX : WY)[p] = val;

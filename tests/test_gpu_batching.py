@@ -218,3 +218,41 @@ def test_tridiag_batched_rejects_oversize(sw):
     with pytest.raises(sw.SwError) as e:
         sw.nhswps.tridiag_batched(z, z + 1.0, z, z)
     assert e.value.status == sw._native.SW_ERR_ARG and "33" in str(e.value)
+
+
+def test_async_state_copies_match_sync(sw):
+    """sw_state_set_all_async / sw_state_get_all_async queued around an
+    asynchronous step give the same fields as the synchronous copies and step,
+    for a float32 work field (pn, converted on the device) and float64 fields."""
+    import torch
+    ng, nz, M = 32, 4, 2
+    outs = []
+    for asyn in (False, True):
+        sp = _ensemble(sw, ng, nz, M, sw.SW_MIXED, 90)
+        L = sw._native.lib()
+        n3 = sp.n3 * M
+        fidx = sw._native.FIELD_INDEX
+        dp = sw._native._dp
+        bufs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
+        for k, b in bufs.items():
+            sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(b.data_ptr(), dp), n3))
+            b.mul_(1.0 + 1e-3)  # a changed input to upload
+        res = {k: torch.zeros(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
+        if asyn:
+            for k, b in bufs.items():
+                sw._native.check(L.sw_state_set_all_async(sp.ctx, fidx[k], ctypes.cast(b.data_ptr(), dp), n3))
+            sw._native.check(L.sw_advance_async(sp.ctx, 2, 1))
+            for k, b in res.items():
+                sw._native.check(L.sw_state_get_all_async(sp.ctx, fidx[k], ctypes.cast(b.data_ptr(), dp), n3))
+            sw._native.check(L.sw_sync(sp.ctx))
+        else:
+            for k, b in bufs.items():
+                sw._native.check(L.sw_state_set_all(sp.ctx, fidx[k], ctypes.cast(b.data_ptr(), dp), n3))
+            sw._native.check(L.sw_advance(sp.ctx, 2, 1))
+            for k, b in res.items():
+                sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(b.data_ptr(), dp), n3))
+        outs.append({k: v.numpy().copy() for k, v in res.items()})
+        sp.close()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+        assert np.any(outs[0][k] != 0.0), k
