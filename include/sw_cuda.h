@@ -145,6 +145,16 @@ int sw_diagnose(sw_ctx* ctx, int member, double out[4]);
 int sw_diag_history(sw_ctx* ctx, double* out, int cap, int* count);
 /* Energies of savegrid (src/nhswps/mod.rs:365-410) of one member: {ekin, epot, etot}. */
 int sw_energy(sw_ctx* ctx, int member, double out[3]);
+/* savegrid's data for one member in one call (src/nhswps/mod.rs:347-663), computed
+ * on the device: energies = {ekin, epot, etot}; spectra = the level-weighted
+ * shell spectra of zeta, delta and gamma times spmf, 3 blocks of kmax+1 values
+ * (nspec = 3*(kmax+1); kmax from sw_spectral_get "kmax"); fields3 = float32
+ * q, delta, gamma (physical), r, w, p, 6 blocks of ng*ng*(nz+1) in Fortran order;
+ * fields2 = float32 -w/z, weighted vorticity, PV, weighted gamma and h at the
+ * top level, 5 blocks of ng*ng.  The caller writes the reference's text and .r4
+ * records from these. */
+int sw_savegrid(sw_ctx* ctx, int member, double energies[3], double* spectra, int nspec, float* fields3,
+                float* fields2);
 /* psolve sweep counts of the last advance step for member 0 (3 entries). */
 int sw_last_sweeps(sw_ctx* ctx, int out[3]);
 /* advance without waiting: queues nsteps graph-captured steps on the context's

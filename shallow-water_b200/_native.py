@@ -66,6 +66,7 @@ _SIGS = {
     "sw_set_graphs": (_i, [_vp, _i]),
     "sw_set_fft_chunk": (_i, [_vp, _i, _ip]),
     "sw_advance_async": (_i, [_vp, _i, _i]),
+    "sw_savegrid": (_i, [_vp, _i, _dp, _dp, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "sw_state_set_all_async": (_i, [_vp, _i, _dp, _sz]),
     "sw_state_get_all_async": (_i, [_vp, _i, _dp, _sz]),
     "sw_tridiag_batched": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),

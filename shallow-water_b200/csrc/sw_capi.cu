@@ -529,21 +529,26 @@ int sw_spctop3d(sw_ctx* ctx, const double* fs, double* fp, int izbeg, int izend)
     return with_solver(ctx, [&](auto& s) { return sw::capi::t3d_impl(s, fs, fp, izbeg, izend, false); });
 }
 
-// spec1d is an output-only diagnostic of savegrid; computed on the host.
+// spec1d (src/spectral/mod.rs:559-591): shell sums on the device, deterministic.
 int sw_spec1d(sw_ctx* ctx, const double* ss, double* spec) {
     return with_solver(ctx, [&](auto& s) {
         require(ss && spec, SW_ERR_ARG, "null array");
-        const int ng = s.ng;
-        const auto& km = s.host.kmag;
-        for (int k = 0; k <= s.host.kmax; k++) spec[k] = 0.0;
-        spec[km[0]] += (1.0 / 4.0) * ss[0] * ss[0];
-        for (int kx = 1; kx < ng; kx++) spec[km[kx]] += (1.0 / 2.0) * ss[kx] * ss[kx];
-        for (int ky = 1; ky < ng; ky++) spec[km[(size_t)ng * ky]] += (1.0 / 2.0) * ss[(size_t)ng * ky] * ss[(size_t)ng * ky];
-        for (int ky = 1; ky < ng; ky++)
-            for (int kx = 1; kx < ng; kx++) {
-                const double v = ss[kx + (size_t)ng * ky];
-                spec[km[kx + (size_t)ng * ky]] += v * v;
-            }
+        const int nb = s.host.kmax + 1;
+        double* tmp = s.WD(11);
+        SW_CUDA(cudaMemcpyAsync(tmp, ss, sizeof(double) * s.n2, cudaMemcpyHostToDevice, s.st));
+        s.spec1d(tmp, tmp + s.n2);
+        SW_CUDA(cudaMemcpyAsync(spec, tmp + s.n2, sizeof(double) * nb, cudaMemcpyDeviceToHost, s.st));
+        SW_CUDA(cudaStreamSynchronize(s.st));
+        return SW_OK;
+    });
+}
+int sw_savegrid(sw_ctx* ctx, int member, double energies[3], double* spectra, int nspec, float* fields3,
+                float* fields2) {
+    return with_solver(ctx, [&](auto& s) {
+        require(energies && spectra && fields3 && fields2 && member >= 0 && member < s.M, SW_ERR_ARG,
+                "bad savegrid arguments");
+        require(nspec == 3 * (s.host.kmax + 1), SW_ERR_ARG, "spectra needs 3*(kmax+1) values");
+        s.savegrid(member, energies, spectra, fields3, fields2);
         return SW_OK;
     });
 }

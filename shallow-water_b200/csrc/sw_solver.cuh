@@ -29,9 +29,10 @@ inline void upload(DevBuf<double>& d, const std::vector<double>& h) {
 }
 
 // Second pass of the pressure sweep's p, p_x, p_y transforms: output o of a chunk
-// is (member mm, kind, level iz), o = (mm * 3 + kind) * nz + iz; kinds 0 and 2 read
-// the intermediates of p and p_y, kind 1 reads p's with kx mirrored and the d/dx
-// factor (src/sta2dfft.rs:128-155).  Columns (iy) are contiguous on both sides.
+// is (member mm, level iz, kind), o = mm * 3 nz + 3 iz + kind, and first-pass plane
+// mm * 2 nz + 2 iz + (0 for p, 1 for p_y); kinds 0 and 2 read the intermediates of
+// p and p_y, kind 1 reads p's with kx mirrored and the d/dx factor
+// (src/sta2dfft.rs:128-155).  Columns (iy) are contiguous on both sides.
 template <typename T>
 struct SweepMidLoad {
     using T2 = typename C2<T>::t;
@@ -39,8 +40,8 @@ struct SweepMidLoad {
     const T* mid;
     int ng, nz;
     __device__ __forceinline__ const T* row(int o, int kx, double& f) const {
-        const int mm = o / (3 * nz), k = o - mm * 3 * nz, kind = k / nz, iz = k - kind * nz;
-        const int plane = mm * 2 * nz + (kind == 2 ? nz : 0) + iz;
+        const int mm = o / (3 * nz), k = o - mm * 3 * nz, iz = k / 3, kind = k - 3 * iz;
+        const int plane = mm * 2 * nz + 2 * iz + (kind == 2 ? 1 : 0);
         f = kind == 1 ? dmul(kx, ng) : 1.0;
         return mid + ((size_t)plane * ng + (kind == 1 ? mirror(kx, ng) : kx)) * ng;
     }
@@ -65,7 +66,7 @@ struct SweepPhysStore {
     T *A, *B, *C;
     int ng, nz, L, m0;
     __device__ __forceinline__ T* dst(int o, int c, int p) const {
-        const int mm = o / (3 * nz), k = o - mm * 3 * nz, kind = k / nz, iz = k - kind * nz;
+        const int mm = o / (3 * nz), k = o - mm * 3 * nz, iz = k / 3, kind = k - 3 * iz;
         T* base = kind == 0 ? A : kind == 1 ? B : C;
         return base + ((size_t)((m0 + mm) * L + iz) * ng + p) * ng + c;
     }
@@ -77,6 +78,24 @@ struct SweepPhysStore {
         *reinterpret_cast<T2*>(dst(o, c, p)) = v;
     }
 };
+
+// Shell spectrum (spec1d, src/spectral/mod.rs:559-591) by bins of |k|: one warp
+// per bin sums wt[e] * src(e) over the bin's elements e (a CSR list built once
+// from kmag) in a fixed order, then a fixed shuffle tree: deterministic.
+template <class SRC>
+__global__ void k_spec_bins(int nbins, const int* __restrict__ off, const int* __restrict__ idx,
+                            const double* __restrict__ wt, SRC src, double* __restrict__ out) {
+    const int bin = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (bin >= nbins) return;
+    double a = 0.0;
+    for (int k = off[bin] + lane; k < off[bin + 1]; k += 32) {
+        const int e = idx[k];
+        a += wt[e] * src(e);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) out[bin] = a;
+}
 
 constexpr int UPDATE_THREADS = 128;
 
@@ -302,35 +321,31 @@ __global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, 
                               int mixed, int nitmax, int use_cond, cudaGraphConditionalHandle cond,
                               long long* nexec) {
     __shared__ int any;
-    __shared__ double sh[2][CTRL_THREADS];
     __shared__ double sums[2 * CTRL_MAX_MEMBERS];
     if (threadIdx.x == 0) any = 0;
-    // per member: strided partial sums, then a fixed-order tree (deterministic)
+    // one warp per member: lane-strided partial sums, then a fixed shuffle tree
+    // (deterministic order)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = CTRL_THREADS / 32;
     for (int m0 = 0; m0 < M; m0 += CTRL_MAX_MEMBERS) {
         const int mcount = (M - m0 < CTRL_MAX_MEMBERS) ? M - m0 : CTRL_MAX_MEMBERS;
-        for (int mm = 0; mm < mcount; mm++) {
-            const int m = m0 + mm;
+        for (int mm = warp; mm < mcount; mm += nwarps) {
+            const double* pm = part + (size_t)(m0 + mm) * nblk * 2;
             double a = 0.0, b = 0.0;
-            for (int k = threadIdx.x; k < nblk; k += CTRL_THREADS) {
-                a += part[((size_t)m * nblk + k) * 2];
-                b += part[((size_t)m * nblk + k) * 2 + 1];
+            for (int k = lane; k < nblk; k += 32) {
+                a += pm[2 * k];
+                b += pm[2 * k + 1];
             }
-            sh[0][threadIdx.x] = a;
-            sh[1][threadIdx.x] = b;
-            __syncthreads();
-            for (int w = CTRL_THREADS / 2; w > 0; w >>= 1) {
-                if (threadIdx.x < w) {
-                    sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
-                    sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
-                }
-                __syncthreads();
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                a += __shfl_down_sync(0xffffffffu, a, off);
+                b += __shfl_down_sync(0xffffffffu, b, off);
             }
-            if (threadIdx.x == 0) {
-                sums[2 * mm] = sh[0][0];
-                sums[2 * mm + 1] = sh[1][0];
+            if (lane == 0) {
+                sums[2 * mm] = a;
+                sums[2 * mm + 1] = b;
             }
-            __syncthreads();
         }
+        __syncthreads();
         for (int mm = threadIdx.x; mm < mcount; mm += CTRL_THREADS) ctrl_member(m0 + mm, sums[2 * mm], sums[2 * mm + 1],
                                                                                  ctl, errp, toler, mixed, nitmax, &any);
         __syncthreads();
@@ -366,6 +381,10 @@ struct Solver {
     DevBuf<int> ctrl;  // per member: active, iters, status
     double* h_pinned = nullptr;  // host staging for small readbacks
     int hist_cap = 4096;
+    DevBuf<int> bin_off, bin_idx;  // elements of each |k| shell (CSR over kmag)
+    DevBuf<double> bin_wt;         // 1/4 at k = 0, 1/2 on the axes, 1 elsewhere
+    DevBuf<double> spec_d;         // 3 (kmax + 1) spectra
+    DevBuf<float> snap;            // savegrid output staging: 6 n3 + 5 n2 floats
     // whole-step CUDA graphs (index: ggen) with device-side psolve loops
     cudaStream_t st_body = nullptr;
     cudaGraphExec_t step_exec[2] = {nullptr, nullptr};
@@ -396,6 +415,26 @@ struct Solver {
         upload(op.weight, host.weight); upload(op.theta, host.theta);
         upload(op.htd1, host.htd1); upload(op.etd1, host.etd1);
         fft.init(ng, 6 * ML);
+        {
+            const int nb = host.kmax + 1;
+            std::vector<int> cnt(nb + 1, 0), off(nb + 1, 0), idx(n2);
+            std::vector<double> wt_h(n2);
+            for (int e = 0; e < n2; e++) cnt[host.kmag[e]]++;
+            for (int k = 0; k < nb; k++) off[k + 1] = off[k] + cnt[k];
+            std::vector<int> pos(off.begin(), off.end());
+            for (int e = 0; e < n2; e++) idx[pos[host.kmag[e]]++] = e;
+            for (int e = 0; e < n2; e++) {
+                const int kx = e % ng, ky = e / ng;
+                wt_h[e] = (kx == 0 && ky == 0) ? 0.25 : (kx == 0 || ky == 0) ? 0.5 : 1.0;
+            }
+            bin_off.alloc(nb + 1);
+            bin_idx.alloc(n2);
+            bin_wt.alloc(n2);
+            SW_CUDA(cudaMemcpy(bin_off.p, off.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice));
+            SW_CUDA(cudaMemcpy(bin_idx.p, idx.data(), sizeof(int) * n2, cudaMemcpyHostToDevice));
+            upload(bin_wt, wt_h);
+            spec_d.alloc((size_t)3 * nb);
+        }
         for (auto* b : {&u, &v, &w, &z, &zx, &zy, &r, &ri, &aa, &zeta, &pn, &dpn, &sigx, &sigy, &cpt1, &cpt2, &sp0}) {
             b->alloc(nf);
             SW_CUDA(cudaMemset(b->p, 0, nf * sizeof(T)));
@@ -1415,8 +1454,8 @@ struct Solver {
         for (int m0 = 0; m0 < M; m0 += mchunk) {
             const int mc = std::min(mchunk, M - m0);
             launch_pass<T, true, true, false>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, n2z * mc, ng,
-                [=] __device__(int o, int kx, int ky) -> T {
-                    const int mm = o / n2z, k = o - mm * n2z, kind = k / nz, iz = k - kind * nz;
+                [=] __device__(int o, int kx, int ky) -> T {  // p, p_y of one level adjacent
+                    const int mm = o / n2z, k = o - mm * n2z, iz = k >> 1, kind = k & 1;
                     const double* pc = PS + (size_t)((m0 + mm) * L + iz) * n2;
                     if (kind == 0) return (T)pc[kx + ng * ky];
                     return (T)(dmul(ky, ng) * pc[kx + ng * mirror(ky, ng)]);
@@ -1778,6 +1817,110 @@ struct Solver {
     }
 
     // energies of savegrid (src/nhswps/mod.rs:365-410)
+    // Spectrum of one float64 spectral plane on the device into out (kmax + 1).
+    void spec1d(const double* ss, double* out) {
+        const int nb = host.kmax + 1;
+        k_spec_bins<<<(nb * 32 + 255) / 256, 256, 0, st>>>(nb, bin_off.p, bin_idx.p, bin_wt.p,
+            [=] __device__(int e) { return ss[e] * ss[e]; }, out);
+        SW_CHECK_LAUNCH();
+        count_launch();
+    }
+
+    // savegrid's data for one member (src/nhswps/mod.rs:347-663), all on the device:
+    // energies (ekin, epot, etot); the level-weighted shell spectra of zeta, delta,
+    // gamma times spmf (3 (kmax + 1) values); the float32 snapshots q, delta,
+    // gamma (physical), r, w, p (6 n3) and the 2-D fields -w/z(nz), the vertically
+    // weighted vorticity and PV, gamma and h (5 n2).  One device-to-host copy.
+    void savegrid(int member, double* energies, double* spectra, float* out3, float* out2) {
+        energy(member, energies);
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, nb = host.kmax + 1;
+        const size_t n3 = (size_t)L * n2;
+        if (!snap.p) snap.alloc(6 * n3 + 5 * (size_t)n2);
+        const size_t mb = (size_t)member * n3;
+        const double *QS = qs.p + mb, *DS = ds.p + mb, *GS = gs.p + mb, *wgt = op.weight;
+        const T *ZE = zeta.p + mb, *R = r.p + mb, *WW = w.p + mb, *Z = z.p + mb, *PN = pn.p + mb;
+        T *ZS = W(0), *GP = W(1);
+        float* S = snap.p;
+        double* SPEC = spec_d.p;
+        // zeta to spectral space (per level)
+        fft.ptospc(st, L, [=] __device__(int q, int iy, int ix) -> T { return ZE[(size_t)q * n2 + iy + ng * ix]; },
+                   [=] __device__(int q, int kx, int ky, T val) { ZS[(size_t)q * n2 + kx + ng * ky] = val; });
+        k_spec_bins<<<(nb * 32 + 255) / 256, 256, 0, st>>>(nb, bin_off.p, bin_idx.p, bin_wt.p,
+            [=] __device__(int e) {
+                double a = 0.0;
+                for (int iz = 0; iz < L; iz++) {
+                    const double v = ZS[(size_t)iz * n2 + e];
+                    a += wgt[iz] * (v * v);
+                }
+                return a;
+            }, SPEC);
+        SW_CHECK_LAUNCH();
+        count_launch();
+        k_spec_bins<<<(nb * 32 + 255) / 256, 256, 0, st>>>(nb, bin_off.p, bin_idx.p, bin_wt.p,
+            [=] __device__(int e) {
+                double a = 0.0;
+                for (int iz = 0; iz < L; iz++) {
+                    const double v = DS[(size_t)iz * n2 + e];
+                    a += wgt[iz] * (v * v);
+                }
+                return a;
+            }, SPEC + nb);
+        SW_CHECK_LAUNCH();
+        count_launch();
+        k_spec_bins<<<(nb * 32 + 255) / 256, 256, 0, st>>>(nb, bin_off.p, bin_idx.p, bin_wt.p,
+            [=] __device__(int e) {
+                double a = 0.0;
+                for (int iz = 0; iz < L; iz++) {
+                    const double v = GS[(size_t)iz * n2 + e];
+                    a += wgt[iz] * (v * v);
+                }
+                return a;
+            }, SPEC + 2 * nb);
+        SW_CHECK_LAUNCH();
+        count_launch();
+        // q, delta, gamma to physical space (float32 snapshots; gamma also kept in T)
+        fft.spctop(st, 3 * L,
+            [=] __device__(int o, int kx, int ky) -> T {
+                const int which = o / L, iz = o - which * L;
+                return (T)(which == 0 ? QS : which == 1 ? DS : GS)[(size_t)iz * n2 + kx + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, T val) {
+                const size_t p = (size_t)o * n2 + iy + ng * ix;
+                S[p] = (float)val;
+                if (o >= 2 * L) GP[p - 2 * n3] = val;
+            });
+        for_planes(st, 3 * L, n2, [=] __device__(int q, int i) {
+            const int which = q / L;
+            const size_t p = (size_t)(q - which * L) * n2 + i;
+            const T* src = which == 0 ? R : which == 1 ? WW : PN;
+            S[3 * n3 + (size_t)q * n2 + i] = (float)src[p];
+        });
+        float* S2 = S + 6 * n3;
+        for_cols(st, n2, [=] __device__(int i) {
+            const double zt = (double)Z[(size_t)nz * n2 + i];
+            double wz = 0.0, wg = 0.0;
+            for (int iz = 0; iz < L; iz++) {
+                const size_t p = (size_t)iz * n2 + i;
+                const double f = 1.0 + (double)R[p];
+                wz += wgt[iz] * (double)ZE[p] * f;
+                wg += wgt[iz] * (double)GP[p] * f;
+            }
+            wz *= HBAR / zt;
+            wg *= HBAR / zt;
+            S2[i] = (float)(-(double)WW[(size_t)nz * n2 + i] / zt);
+            S2[n2 + i] = (float)wz;
+            S2[2 * (size_t)n2 + i] = (float)(HBAR * (wz + COF) / zt - COF);
+            S2[3 * (size_t)n2 + i] = (float)wg;
+            S2[4 * (size_t)n2 + i] = (float)((1.0 / HBAR) * zt - 1.0);
+        });
+        SW_CUDA(cudaMemcpyAsync(spectra, SPEC, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaMemcpyAsync(out3, S, sizeof(float) * 6 * n3, cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaMemcpyAsync(out2, S2, sizeof(float) * 5 * (size_t)n2, cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaStreamSynchronize(st));
+        for (int k = 0; k < nb; k++)
+            for (int j = 0; j < 3; j++) spectra[j * nb + k] *= host.spmf[k];
+    }
+
     void energy(int member, double* out3) {
         const int n2 = this->n2, L = this->L, nz = this->nz;
         T *R = r, *U = u, *V = v, *WW = w, *Z = z;

@@ -189,7 +189,10 @@ def last_sweeps(spectral):
 
 # ---- run driver and output (src/nhswps/mod.rs:32-85, 150-663) -----------------------
 class Output:
-    """The 14 output files of nhswps (src/nhswps/mod.rs:32-85)."""
+    """The 14 output files of nhswps (src/nhswps/mod.rs:32-85).  The float32
+    snapshot records of savegrid are appended by one background writer thread in
+    submission order (`flush()`/`close()` wait for it), so the time loop does not
+    wait for file I/O."""
 
     NAMES = {
         "ecomp": "ecomp.asc", "monitor": "monitor.asc", "spectra": "spectra.asc",
@@ -200,6 +203,8 @@ class Output:
 
     def __init__(self, files):
         self.__dict__.update(files)
+        self._pool = None
+        self._pending = []
 
     @classmethod
     def from_path(cls, path):
@@ -210,7 +215,23 @@ class Output:
             files[k] = open(os.path.join(path, rel), "w" if rel.endswith(".asc") else "wb")
         return cls(files)
 
+    def submit(self, fn, *args):
+        """Run fn(*args) on the writer thread (in order)."""
+        if self._pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=1)
+        self._pending.append(self._pool.submit(fn, *args))
+
+    def flush(self):
+        for f in self._pending:
+            f.result()
+        self._pending = []
+
     def close(self):
+        self.flush()
+        if self._pool is not None:
+            self._pool.shutdown()
+            self._pool = None
         for k in self.NAMES:
             getattr(self, k).close()
 
@@ -220,54 +241,52 @@ def _append_r4(f, t, data):
     f.write(np.asarray(data, dtype="<f4").reshape(-1, order="F").tobytes(order="F"))
 
 
-def savegrid(state, output):
-    """Energies, spectra and f32 snapshots at a save time (src/nhswps/mod.rs:347-663)."""
+def savegrid_data(state):
+    """savegrid's numbers computed on the device in one call (sw_savegrid):
+    (energies[3], spectra (3, kmax+1), fields3 {name: float32 flat}, fields2
+    {name: float32 flat})."""
     sp = state.spectral
-    ng, nz = sp.ng, sp.nz
+    n2, n3 = sp.n2, sp.n3
+    nb = sp.kmax + 1
+    energies = np.zeros(3)
+    spectra = np.zeros(3 * nb)
+    f3 = np.zeros(6 * n3, dtype=np.float32)
+    f2 = np.zeros(5 * n2, dtype=np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    check(lib().sw_savegrid(sp.ctx, state.member, dptr(energies), dptr(spectra), 3 * nb,
+                            f3.ctypes.data_as(fp), f2.ctypes.data_as(fp)))
+    names3 = ("qs", "ds", "gs", "r", "w", "pn")
+    names2 = ("d", "zeta", "q", "g", "h")
+    return (energies, spectra.reshape(3, nb), {k: f3[i * n3:(i + 1) * n3] for i, k in enumerate(names3)},
+            {k: f2[i * n2:(i + 1) * n2] for i, k in enumerate(names2)})
+
+
+def _write_records(output, t, f3, f2):
+    for key, name in (("d3ql", "qs"), ("d3d", "ds"), ("d3g", "gs"), ("d3r", "r"), ("d3w", "w"), ("d3pn", "pn")):
+        _append_r4(getattr(output, key), t, f3[name])
+    for key, name in (("d2d", "d"), ("d2zeta", "zeta"), ("d2q", "q"), ("d2g", "g"), ("d2h", "h")):
+        _append_r4(getattr(output, key), t, f2[name])
+
+
+def savegrid(state, output):
+    """Energies, spectra and f32 snapshots at a save time (src/nhswps/mod.rs:347-663).
+    The numbers come from the device in one call; the text lines are written here
+    and the binary records by the output's writer thread."""
+    sp = state.spectral
     t = state.t
-    ekin, epot, etot = energy(state)
+    (ekin, epot, etot), spec, f3, f2 = savegrid_data(state)
     output.ecomp.write("%.6f %.9f %.9f %.9f %.9f %.9f\n" % (t, 0.0, ekin, ekin, epot, etot))
-    f = {k: state.get(k) for k in ("qs", "ds", "gs", "r", "w", "pn", "z", "zeta")}
-    weight = sp.weight
-    zspec = np.zeros(ng + 1)
-    dspec = np.zeros(ng + 1)
-    gspec = np.zeros(ng + 1)
-    for iz in range(nz + 1):
-        zspec += weight[iz] * sp.spec1d(sp.ptospc(f["zeta"][:, :, iz]))
-        dspec += weight[iz] * sp.spec1d(f["ds"][:, :, iz])
-        gspec += weight[iz] * sp.spec1d(f["gs"][:, :, iz])
-    spmf = sp.spmf
-    zspec *= spmf
-    dspec *= spmf
-    gspec *= spmf
+    zspec, dspec, gspec = spec
     output.spectra.write("%.6f %d\n" % (t, sp.kmaxred))
     alk = sp.alk
     with np.errstate(divide="ignore"):
         for k in range(1, sp.kmaxred + 1):
             output.spectra.write("%.8f %.8f %.8f %.8f\n" % (alk[k - 1], np.log10(zspec[k]),
                                                           np.log10(dspec[k] + 1.0e-32), np.log10(gspec[k] + 1.0e-32)))
-    L = nz + 1
-    for key, out in (("qs", output.d3ql), ("ds", output.d3d), ("gs", output.d3g)):
-        phys = sp.spctop3d(f[key], np.zeros((ng, ng, L), order="F"), 0, nz)
-        _append_r4(out, t, phys)
-    _append_r4(output.d3r, t, f["r"])
-    _append_r4(output.d3w, t, f["w"])
-    _append_r4(output.d3pn, t, f["pn"])
-    zt = f["z"][:, :, nz]
-    _append_r4(output.d2d, t, -f["w"][:, :, nz] / zt)
-    wkp = np.zeros((ng, ng), order="F")
-    for iz in range(L):
-        wkp += weight[iz] * f["zeta"][:, :, iz] * (1.0 + f["r"][:, :, iz])
-    wkp *= HBAR / zt
-    _append_r4(output.d2zeta, t, wkp)
-    _append_r4(output.d2q, t, HBAR * (wkp + COF) / zt - COF)
-    gphys = sp.spctop3d(f["gs"], np.zeros((ng, ng, L), order="F"), 0, nz)
-    wkp = np.zeros((ng, ng), order="F")
-    for iz in range(L):
-        wkp += weight[iz] * gphys[:, :, iz] * (1.0 + f["r"][:, :, iz])
-    wkp *= HBAR / zt
-    _append_r4(output.d2g, t, wkp)
-    _append_r4(output.d2h, t, (1.0 / HBAR) * zt - 1.0)
+    if hasattr(output, "submit"):
+        output.submit(_write_records, output, t, f3, f2)
+    else:
+        _write_records(output, t, f3, f2)
 
 
 def _round_half_away(x):
