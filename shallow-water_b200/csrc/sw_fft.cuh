@@ -566,13 +566,16 @@ inline size_t fft_pass_smem_r() {
 // Four twiddles come from the table (r = 1, 2, 4, 8); the other eleven are
 // products of at most three of them, which keeps shared-memory instructions (the
 // pass's limiting pipe) down at a cost of a few roundings per twiddle.
+// tw4 holds exp(-2 pi i m j / 256) for m = 1, 2, 4, 8 and j < 16 as four rows of
+// 16, so that the sixteen threads of a butterfly row read consecutive entries
+// (no shared-memory bank conflicts, unlike strided reads of the full table).
 template <bool INV, typename T2>
-__device__ __forceinline__ void stage2_16x16(T2* v, const T2* __restrict__ tw, int j) {
+__device__ __forceinline__ void stage2_16x16(T2* v, const T2* __restrict__ tw4, int j) {
     T2 w[16];
-    w[1] = tw[j];
-    w[2] = tw[2 * j];
-    w[4] = tw[4 * j];
-    w[8] = tw[8 * j];
+    w[1] = tw4[j];
+    w[2] = tw4[16 + j];
+    w[4] = tw4[32 + j];
+    w[8] = tw4[48 + j];
     w[3] = cmul(w[1], w[2]);
     w[5] = cmul(w[1], w[4]);
     w[6] = cmul(w[2], w[4]);
@@ -601,12 +604,12 @@ k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
     static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
     constexpr int N = FFT_R_N, H = N / 2, NP = FFT_R_NP, PL = FFT_R_PL, TC = 2 * NP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T2* tw = reinterpret_cast<T2*>(smem_raw);
+    T2* tw = reinterpret_cast<T2*>(smem_raw);  // 64 entries: the rows of stage2_16x16
     T2* buf = tw + N;
     const int tid = threadIdx.x;
     const int o = blockIdx.y;
     const int c0 = blockIdx.x * TC;
-    tw[tid] = twg[tid];
+    if (tid < 64) tw[tid] = twg[(1 << (tid >> 4)) * (tid & 15)];
     // (pair, butterfly) with the pair index on the lanes (column-contiguous global
     // access) or the butterfly index on the lanes (point-contiguous access, and the
     // conflict-free order of the in-place shared-memory stage)

@@ -97,6 +97,33 @@ __global__ void k_spec_bins(int nbins, const int* __restrict__ off, const int* _
     if (lane == 0) out[bin] = a;
 }
 
+// dp/dtheta of psolve's finish (psolve.rs:371-410) for one (kx, ky) column with
+// nz = NZS at compile time: the column of ps and the compact-scheme unknowns stay
+// in registers (same arithmetic as the streamed loop in psolve_finish).
+template <typename T, int NZS>
+__global__ void __launch_bounds__(128)
+k_dpdtheta(int n2, int ncols, const double* __restrict__ PS, const T* __restrict__ SP, const double* __restrict__ htd1,
+           const double* __restrict__ etd1, double hdzi, double dzi, double dz6, double* __restrict__ GG) {
+    const int c = blockIdx.x * 128 + threadIdx.x;
+    if (c >= ncols) return;
+    const int m = c / n2, i = c - m * n2;
+    const size_t cb = (size_t)m * (NZS + 1) * n2 + i;
+    double p[NZS + 1], g[NZS + 1];
+#pragma unroll
+    for (int iz = 0; iz <= NZS; iz++) p[iz] = PS[cb + (size_t)iz * n2];
+    const double spn = (double)SP[cb + (size_t)NZS * n2];
+    g[0] = 0.0;
+    g[1] = (p[2] - p[0]) * hdzi * htd1[0];
+#pragma unroll
+    for (int iz = 2; iz < NZS; iz++) g[iz] = ((p[iz + 1] - p[iz - 1]) * hdzi - (1.0 / 6.0) * g[iz - 1]) * htd1[iz - 1];
+    const double gn = dz6 * spn - p[NZS - 1] * dzi;
+    g[NZS] = (gn - (1.0 / 3.0) * g[NZS - 1]) * htd1[NZS - 1];
+#pragma unroll
+    for (int iz = NZS - 1; iz >= 1; iz--) g[iz] = g[iz] + etd1[iz - 1] * g[iz + 1];
+#pragma unroll
+    for (int iz = 1; iz <= NZS; iz++) GG[cb + (size_t)iz * n2] = g[iz];
+}
+
 constexpr int UPDATE_THREADS = 128;
 
 // Semi-implicit update of one (kx, ky) column (advance.rs:60-279; the same
@@ -1546,7 +1573,19 @@ struct Solver {
         (void)htdv; (void)etdv; (void)ap; (void)dz2; (void)dzisq; (void)hdzi; (void)mixed;
         // dp/dtheta by 4th-order compact differences (psolve.rs:371-410), levels 1..nz
         double* GG = WD(1);
-        for_cols(st, M * n2, [=] __device__(int c) {
+        const int ncols = M * n2, nbk = (ncols + 127) / 128;
+        bool done = true;
+        switch (nz) {
+            case 4: k_dpdtheta<T, 4><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            case 8: k_dpdtheta<T, 8><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            case 16: k_dpdtheta<T, 16><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            case 32: k_dpdtheta<T, 32><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            default: done = false;
+        }
+        if (done) {
+            SW_CHECK_LAUNCH();
+            count_launch();
+        } else for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
             const size_t cb = (size_t)m * L * n2 + i;
             auto P = [&](int iz) { return PS[cb + (size_t)iz * n2]; };
