@@ -545,8 +545,8 @@ k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
 }
 
 // ---------------------------------------------------------------------------
-// Register-staged pass for n = 256 = 16 x 16 with 16 column pairs (32 columns)
-// per tile: 256 threads, one radix-16 butterfly each per stage.  The
+// Register-staged pass for n = 256 = 16 x 16 with NP column pairs per tile
+// (fft_r_np): 16 NP threads, one radix-16 butterfly each per stage.  The
 // butterfly next to global memory runs on registers: a forward pass loads the 16
 // points j + 16 r of its pair straight into the first butterfly, and a reverse
 // pass stores the 16 modes j + 16 r of its second butterfly straight to global
@@ -554,11 +554,16 @@ k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
 // two-buffer pass.  The stage that stays in shared memory works in place (each
 // thread reads and writes its own 16 slots), so one tile buffer suffices.
 // ---------------------------------------------------------------------------
-constexpr int FFT_R_N = 256, FFT_R_NP = 16, FFT_R_PL = 256 + 16 + 1;
+constexpr int FFT_R_N = 256, FFT_R_PL = 256 + 16 + 1;
+// Column pairs per tile: 16 (256 threads, 4 CTAs per SM) for float32; 8 (128
+// threads, 4 CTAs per SM) for float64, whose 16-point butterflies need twice the
+// registers (measured 3% faster than 16 pairs at 2 CTAs per SM).
+template <typename T>
+__host__ __device__ constexpr int fft_r_np() { return sizeof(T) == 8 ? 8 : 16; }
 
 template <typename T>
 inline size_t fft_pass_smem_r() {
-    return sizeof(typename C2<T>::t) * ((size_t)FFT_R_N + (size_t)FFT_R_NP * FFT_R_PL);
+    return sizeof(typename C2<T>::t) * ((size_t)FFT_R_N + (size_t)fft_r_np<T>() * FFT_R_PL);
 }
 
 // Second radix-16 stage of 256 = 16 x 16 on the slots j + 16 r of one sequence:
@@ -597,12 +602,12 @@ __device__ __forceinline__ void stage2_16x16(T2* v, const T2* __restrict__ tw4, 
 }
 
 template <typename T, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
-__global__ void __launch_bounds__(FFT_THREADS, sizeof(T) == 8 ? 2 : 4)
+__global__ void __launch_bounds__(16 * fft_r_np<T>(), 4)
 k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
     using T2 = typename C2<T>::t;
     static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
     static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
-    constexpr int N = FFT_R_N, H = N / 2, NP = FFT_R_NP, PL = FFT_R_PL, TC = 2 * NP;
+    constexpr int N = FFT_R_N, H = N / 2, NP = fft_r_np<T>(), PL = FFT_R_PL, TC = 2 * NP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* tw = reinterpret_cast<T2*>(smem_raw);  // 64 entries: the rows of stage2_16x16
     T2* buf = tw + N;

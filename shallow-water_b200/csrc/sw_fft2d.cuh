@@ -131,7 +131,7 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
     // every tile is full (the generic kernel covers the rest)
     constexpr bool pair_ok = INV ? LCF : SCF;
     if constexpr (pair_ok) {
-        if (plan.n == FFT_R_N && tc == 2 * FFT_R_NP && ncols % tc == 0) {
+        if (plan.n == FFT_R_N && tc == 2 * fft_r_np<T>() && ncols % tc == 0) {
             auto kern = k_fft_pass_r<T, INV, LCF, SCF, LD, ST>;
             static int attr_r[64] = {};
             if (dev < 64 && !attr_r[dev]) {
@@ -140,7 +140,7 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
                 attr_r[dev] = 1;
             }
             dim3 grid(ncols / tc, nout);
-            kern<<<grid, FFT_THREADS, fft_pass_smem_r<T>(), s>>>(tw, sc, ld, st);
+            kern<<<grid, 16 * fft_r_np<T>(), fft_pass_smem_r<T>(), s>>>(tw, sc, ld, st);
             SW_CHECK_LAUNCH();
             count_launch();
             return;
@@ -206,8 +206,8 @@ struct Fft2d {
         cap = cap_planes;
         mid.alloc((size_t)cap * ng * ng);
         chunk = default_chunk(ng, cap);
-        // n = 256: the register-staged pass with 32-column tiles (one buffer)
-        tc = ng == FFT_R_N ? 2 * FFT_R_NP : pick_tile<T>(ng);
+        // n = 256: the register-staged pass (16- or 32-column tiles, one buffer)
+        tc = ng == FFT_R_N ? 2 * fft_r_np<T>() : pick_tile<T>(ng);
         sc = (T)(1.0 / std::sqrt((double)ng));
     }
     // Planes per launch pair, clamped to [1, cap]; returns the value in use.

@@ -358,6 +358,7 @@ __global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, 
         for (int mm = warp; mm < mcount; mm += nwarps) {
             const double* pm = part + (size_t)(m0 + mm) * nblk * 2;
             double a = 0.0, b = 0.0;
+#pragma unroll 8
             for (int k = lane; k < nblk; k += 32) {
                 a += pm[2 * k];
                 b += pm[2 * k + 1];
