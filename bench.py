@@ -68,24 +68,60 @@ def algorithmic_bytes_per_step(ng, nz, sweeps, w_fft):
 
 
 class ClockSampler:
-    """Samples nvidia-smi SM clocks and throttle reasons while running."""
+    """Samples the SM clock and the clock-event (throttle) reasons while running:
+    through NVML every 20 ms when it is available (the GPU found by its PCI bus id,
+    so that CUDA_VISIBLE_DEVICES renumbering does not matter), else through
+    nvidia-smi every 200 ms.  Read-only: no setting of the GPU is touched."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []  # (sm_mhz, max_mhz, set of reason names)
         self._stop = threading.Event()
         self._th = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def _run(self):
+        try:
+            nv, h = self._nvml_handle()
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.source = "nvml"
+            while not self._stop.is_set():
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), {k for k, b in bits.items() if r & b}))
+                self._stop.wait(0.02)
+            return
+        except Exception:
+            self.source = "nvidia-smi"
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
                 if out.returncode == 0 and out.stdout.strip():
-                    self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
+                    c = [x.strip() for x in out.stdout.strip().split(",")]
+                    if c[1].replace(".", "").isdigit() and c[2].replace(".", "").isdigit():
+                        reasons = {n for k, n in enumerate(self.NAMES)
+                                   if len(c) > 5 + k and c[5 + k].lower().startswith("active")}
+                        self.rows.append((float(c[1]), float(c[2]), reasons))
             except Exception:
                 pass
             self._stop.wait(0.2)
@@ -101,17 +137,12 @@ class ClockSampler:
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "source": self.source}
         reasons = set()
-        for r in self.rows:
-            for k, name in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        for _, _, r in self.rows:
+            reasons |= r
+        return {"sm_mhz": float(np.median([r[0] for r in self.rows])), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted(reasons), "samples": len(self.rows), "source": self.source}
 
 
 def measured_peak():
