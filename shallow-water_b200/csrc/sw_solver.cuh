@@ -343,7 +343,11 @@ __device__ __forceinline__ void ctrl_member(int m, double a, double b, int* ctl,
 // Convergence control of one sweep (psolve.rs:89, 339-358): per member, the
 // relative change errp from the CTA partials (fixed order), the divergence and
 // iteration-cap statuses, and the mixed path's stop rule; then, inside a graph,
-// the WHILE node's condition (any member still iterating).
+// the WHILE node's condition (any member still iterating).  Stop rule
+// (psolve.rs:17, 89): float64, the reference's 1e-9 on the relative change;
+// float32 transforms put a floor of ~1e-6 under that change, so the mixed path
+// stops at 1e-6, or earlier once the change has stagnated (< 1e-4 and no longer
+// shrinking by 30% per sweep).
 __global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, int* ctl, double* errp, double toler,
                               int mixed, int nitmax, int use_cond, cudaGraphConditionalHandle cond,
                               long long* nexec) {
@@ -1046,18 +1050,9 @@ struct Solver {
             psolve_prepare_fused();
             return;
         }
-        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
-        // Stop rule (psolve.rs:17, 89).  float64 path: the reference's 1e-9 on the
-        // relative change.  float32 transforms put a floor of ~1e-6 under that
-        // change, so the mixed path stops at 1e-6, or earlier once the change has
-        // stagnated (< 1e-4 and no longer shrinking by 30% per sweep).
-        const bool mixed = sizeof(T) == 4;
-        const double toler = mixed ? 1.0E-6 : 1.0E-9;
-        const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz2 = dz / 2.0, dz6 = dz / 6.0;
-        const double dzisq = (1.0 / dz) * (1.0 / dz);
-        const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
-        const double *filt = op.filt, *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap, *htd1 = op.htd1, *etd1 = op.etd1;
-        T *R = r, *RI = ri, *PN = pn, *DPN = dpn;
+        const int ng = this->ng, n2 = this->n2, ML = this->ML;
+        const double* filt = op.filt;
+        T *R = r, *RI = ri, *PN = pn;
         double* PS = ps;
         // ri = 1/(1+r), dealiased
         T* Sr = W(0);
@@ -1073,10 +1068,7 @@ struct Solver {
         vertical();
         coeffs();
         cpsource();
-        T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
-        T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
         int* ctl = ctrl.p;
-        double* errp = errp_d.p;
         // spectral pressure of the first guess, all levels: ps = ptospc(pn).  The sweep
         // reads levels 0..nz-1 only (ps(nz) = 0 in psolve.rs); the first Thomas solve
         // takes ps(nz) into the residual as the previous iterate and then zeroes it.
