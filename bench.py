@@ -310,7 +310,7 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
         outs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs")}
         for k in pinned:
             sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(pinned[k].data_ptr(), sw._native._dp), n3))
-        e2e_steps = max(2, min(args.steps, 5))
+        e2e_steps = max(2, min(args.steps, 10))
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -611,7 +611,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
                     help="precision of the timed (headline) path")
-    ap.add_argument("--members", type=int, default=8, help="ensemble members per GPU (one batched context)")
+    ap.add_argument("--members", type=int, default=16, help="ensemble members per GPU (one batched context)")
     ap.add_argument("--compare", default="on", choices=["on", "off"],
                     help="also time the other precision on the same ensemble and report the ratio and the "
                          "mixed-vs-FP64 rel-L2 after the timed steps")
