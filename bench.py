@@ -353,6 +353,7 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
     for g in range(2):
         sp = sw.Spectral(NG, NZ, precision=prec, nmembers=half, device=local)
         if tune:
+            sp.set_fft_tile(tune["tile"])
             sp.set_fft_chunk(tune["chosen"])
         for j in range(half):
             q3, d3, g3 = initial_fields(NG, NZ, args.seed0 + rank * M + g * half + j, lambda ng: qq2)
@@ -635,7 +636,8 @@ def main():
                     help="time an ensemble of MEMBERS members with ng drawn from {64,96,128,192,256} and nz "
                          "from {4,8,16}: one batched context per (ng, nz) group, groups run concurrently")
     ap.add_argument("--autotune", default="on", choices=["on", "off"],
-                    help="time the 2-D transform launch chunk candidates before warm-up and keep the fastest")
+                    help="time the 2-D transform tile-width and launch-chunk candidates before warm-up and "
+                         "keep the fastest")
     ap.add_argument("--graphs", default="on", choices=["on", "off"],
                     help="run each step as one CUDA graph (on) or host-driven (off; same kernels, for profiling)")
     args = ap.parse_args()

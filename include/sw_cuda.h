@@ -130,13 +130,19 @@ int sw_set_graphs(sw_ctx* ctx, int enable);
  * *in_use (may be NULL) gets the value now in use.  Results do not depend on it.  No reference counterpart:
  * the reference transforms one plane at a time (src/sta2dfft.rs:91-123). */
 int sw_set_fft_chunk(sw_ctx* ctx, int planes, int* in_use);
-/* Autotuner of that chunk: times reps forward + inverse transforms of the
- * pressure sweep's batch (3*nz planes per member) at each candidate (the capacity,
- * halved down to 8 planes), on scratch buffers it allocates, and keeps the
- * fastest.  Up to maxc rows of (chunks[i], ms[i] per transform pair) are written
- * when the arrays are non-NULL; *ncand gets the row count, *chosen the chunk now
- * in use.  No reference counterpart. */
-int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* chunks, float* ms, int* ncand, int* chosen);
+/* Columns per tile of the n = 256 tile passes, 16 or 32 (other lengths have a fixed
+ * tile; columns <= 0 only queries).  *in_use (may be NULL) gets the value now in
+ * use.  Results do not depend on it.  No reference counterpart. */
+int sw_set_fft_tile(sw_ctx* ctx, int columns, int* in_use);
+/* Autotuner of the tile width and the chunk: times reps forward + inverse
+ * transforms of the pressure sweep's batch (3*nz planes per member) for each tile
+ * width the grid has kernels for (n = 256: 16 and 32 columns) and each chunk (the
+ * capacity, halved down to 8 planes), on scratch buffers it allocates, and keeps
+ * the fastest pair.  Up to maxc rows of (tiles[i], chunks[i], ms[i] per transform
+ * pair) are written when the arrays are non-NULL; *ncand gets the row count,
+ * *chosen_tile and *chosen_chunk the values now in use.  No reference counterpart. */
+int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* tiles, int* chunks, float* ms, int* ncand, int* chosen_tile,
+                    int* chosen_chunk);
 /* diagnose (src/nhswps/mod.rs:666-711) of one member:
  * out = {0.5*zrms^2, zrms, zmax, umax}. */
 int sw_diagnose(sw_ctx* ctx, int member, double out[4]);

@@ -71,7 +71,8 @@ _SIGS = {
     "sw_state_get_all_async": (_i, [_vp, _i, _dp, _sz]),
     "sw_tridiag_batched": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "sw_tridiag_batched_host": (_i, [_i, _i, _dp, _dp, _dp, _dp, _dp]),
-    "sw_autotune_fft": (_i, [_vp, _i, _i, _ip, ctypes.POINTER(ctypes.c_float), _ip, _ip]),
+    "sw_autotune_fft": (_i, [_vp, _i, _i, _ip, _ip, ctypes.POINTER(ctypes.c_float), _ip, _ip, _ip]),
+    "sw_set_fft_tile": (_i, [_vp, _i, _ip]),
     "sw_diagnose": (_i, [_vp, _i, _dp]),
     "sw_diag_history": (_i, [_vp, _dp, _i, _ip]),
     "sw_energy": (_i, [_vp, _i, _dp]),

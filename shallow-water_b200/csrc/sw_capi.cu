@@ -722,11 +722,19 @@ int sw_set_fft_chunk(sw_ctx* ctx, int planes, int* in_use) {
         return SW_OK;
     });
 }
-int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* chunks, float* ms, int* ncand, int* chosen) {
+int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* tiles, int* chunks, float* ms, int* ncand, int* chosen_tile,
+                    int* chosen_chunk) {
     if (maxc < 0) return fail(SW_ERR_ARG, "maxc must be >= 0");
     return with_solver(ctx, [&](auto& s) {
-        const int v = s.autotune_fft(reps, maxc, chunks, ms, ncand);
-        if (chosen) *chosen = v;
+        const int v = s.autotune_fft(reps, maxc, tiles, chunks, ms, ncand, chosen_tile);
+        if (chosen_chunk) *chosen_chunk = v;
+        return SW_OK;
+    });
+}
+int sw_set_fft_tile(sw_ctx* ctx, int columns, int* in_use) {
+    return with_solver(ctx, [&](auto& s) {
+        const int v = s.set_fft_tile(columns);
+        if (in_use) *in_use = v;
         return SW_OK;
     });
 }

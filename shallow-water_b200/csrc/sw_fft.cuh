@@ -546,7 +546,7 @@ k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
 
 // ---------------------------------------------------------------------------
 // Register-staged pass for n = 256 = 16 x 16 with NP column pairs per tile
-// (fft_r_np): 16 NP threads, one radix-16 butterfly each per stage.  The
+// (8 or 16): 16 NP threads, one radix-16 butterfly each per stage.  The
 // butterfly next to global memory runs on registers: a forward pass loads the 16
 // points j + 16 r of its pair straight into the first butterfly, and a reverse
 // pass stores the 16 modes j + 16 r of its second butterfly straight to global
@@ -555,15 +555,19 @@ k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
 // thread reads and writes its own 16 slots), so one tile buffer suffices.
 // ---------------------------------------------------------------------------
 constexpr int FFT_R_N = 256, FFT_R_PL = 256 + 16 + 1;
-// Column pairs per tile: 16 (256 threads, 4 CTAs per SM) for float32; 8 (128
-// threads, 4 CTAs per SM) for float64, whose 16-point butterflies need twice the
-// registers (measured 3% faster than 16 pairs at 2 CTAs per SM).
+// Column pairs per tile: 8 or 16, compiled for both and chosen at run time (the
+// autotuner times both).  Default: 16 (256 threads, 4 CTAs per SM) for float32;
+// 8 (128 threads, 4 CTAs per SM) for float64, whose 16-point butterflies need
+// twice the registers (3% faster than 16 pairs at 2 CTAs per SM).
 template <typename T>
 __host__ __device__ constexpr int fft_r_np() { return sizeof(T) == 8 ? 8 : 16; }
+// CTAs per SM the launch bounds ask for (registers per thread <= 65536 / (16 NP MINB))
+template <typename T, int NP>
+__host__ __device__ constexpr int fft_r_minb() { return NP == 8 ? (sizeof(T) == 8 ? 4 : 8) : (sizeof(T) == 8 ? 2 : 4); }
 
 template <typename T>
-inline size_t fft_pass_smem_r() {
-    return sizeof(typename C2<T>::t) * ((size_t)FFT_R_N + (size_t)fft_r_np<T>() * FFT_R_PL);
+inline size_t fft_pass_smem_r(int np) {
+    return sizeof(typename C2<T>::t) * ((size_t)FFT_R_N + (size_t)np * FFT_R_PL);
 }
 
 // Second radix-16 stage of 256 = 16 x 16 on the slots j + 16 r of one sequence:
@@ -601,13 +605,13 @@ __device__ __forceinline__ void stage2_16x16(T2* v, const T2* __restrict__ tw4, 
     butterfly<16, INV>(v);
 }
 
-template <typename T, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
-__global__ void __launch_bounds__(16 * fft_r_np<T>(), 4)
+template <typename T, int NPT, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
+__global__ void __launch_bounds__(16 * NPT, fft_r_minb<T, NPT>())
 k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
     using T2 = typename C2<T>::t;
     static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
     static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
-    constexpr int N = FFT_R_N, H = N / 2, NP = fft_r_np<T>(), PL = FFT_R_PL, TC = 2 * NP;
+    constexpr int N = FFT_R_N, H = N / 2, NP = NPT, PL = FFT_R_PL, TC = 2 * NP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* tw = reinterpret_cast<T2*>(smem_raw);  // 64 entries: the rows of stage2_16x16
     T2* buf = tw + N;

@@ -123,7 +123,7 @@ template <typename T, bool INV, bool LCF, bool SCF, class LD, class ST>
 inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T>::t* tw, int tc, T sc,
                         int nout, int ncols, LD ld, ST st) {
     if (nout <= 0) return;
-    constexpr int LT256 = sizeof(T) == 8 ? 4 : 5, LT128 = 5;
+    constexpr int LT128 = 5;
     const size_t smem = fft_pass_smem<T>(plan.n, tc);
     int dev = 0;
     cudaGetDevice(&dev);
@@ -131,31 +131,31 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
     // every tile is full (the generic kernel covers the rest)
     constexpr bool pair_ok = INV ? LCF : SCF;
     if constexpr (pair_ok) {
-        if (plan.n == FFT_R_N && tc == 2 * fft_r_np<T>() && ncols % tc == 0) {
-            auto kern = k_fft_pass_r<T, INV, LCF, SCF, LD, ST>;
-            static int attr_r[64] = {};
-            if (dev < 64 && !attr_r[dev]) {
+        if (plan.n == FFT_R_N && (tc == 16 || tc == 32) && ncols % tc == 0) {
+            const int np = tc / 2;
+            auto kern = np == 8 ? k_fft_pass_r<T, 8, INV, LCF, SCF, LD, ST> : k_fft_pass_r<T, 16, INV, LCF, SCF, LD, ST>;
+            static int attr_r[64][2] = {};
+            if (dev < 64 && !attr_r[dev][np == 8 ? 0 : 1]) {
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-                attr_r[dev] = 1;
+                attr_r[dev][np == 8 ? 0 : 1] = 1;
             }
             dim3 grid(ncols / tc, nout);
-            kern<<<grid, 16 * fft_r_np<T>(), fft_pass_smem_r<T>(), s>>>(tw, sc, ld, st);
+            kern<<<grid, 16 * np, fft_pass_smem_r<T>(np), s>>>(tw, sc, ld, st);
             SW_CHECK_LAUNCH();
             count_launch();
             return;
         }
     }
     if constexpr (pair_ok) {
-        const bool s256 = plan.n == 256 && tc == (1 << LT256), s128 = plan.n == 128 && tc == (1 << LT128);
-        if ((s256 || s128) && ncols % tc == 0) {
-            auto kern = s256 ? k_fft_pass_s<T, 256, LT256, INV, LCF, SCF, LD, ST>
-                             : k_fft_pass_s<T, 128, LT128, INV, LCF, SCF, LD, ST>;
-            static int attr_s[64][2] = {};
-            if (dev < 64 && !attr_s[dev][s256 ? 0 : 1]) {
+        // n = 128 (n = 256 tiles are all served by the register-staged pass above)
+        if (plan.n == 128 && tc == (1 << LT128) && ncols % tc == 0) {
+            auto kern = k_fft_pass_s<T, 128, LT128, INV, LCF, SCF, LD, ST>;
+            static int attr_s[64] = {};
+            if (dev < 64 && !attr_s[dev]) {
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-                attr_s[dev][s256 ? 0 : 1] = 1;
+                attr_s[dev] = 1;
             }
             dim3 grid(ncols / tc, nout);
             kern<<<grid, FFT_THREADS, smem, s>>>(tw, sc, ld, st);
@@ -209,6 +209,12 @@ struct Fft2d {
         // n = 256: the register-staged pass (16- or 32-column tiles, one buffer)
         tc = ng == FFT_R_N ? 2 * fft_r_np<T>() : pick_tile<T>(ng);
         sc = (T)(1.0 / std::sqrt((double)ng));
+    }
+    // Columns per tile of the n = 256 passes: 16 or 32 (other lengths keep their
+    // fixed tile); returns the value in use.
+    int set_tile(int columns) {
+        if (ng == FFT_R_N && (columns == 16 || columns == 32)) tc = columns;
+        return tc;
     }
     // Planes per launch pair, clamped to [1, cap]; returns the value in use.
     int set_chunk(int planes) {

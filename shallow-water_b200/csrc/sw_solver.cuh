@@ -520,13 +520,27 @@ struct Solver {
         return fft.set_chunk(planes);
     }
 
+    // Columns per tile of the n = 256 tile passes (16 or 32); like the chunk, the
+    // captured step graphs hold the old launches, so they are dropped.
+    int set_fft_tile(int columns) {
+        if (columns <= 0 || columns == fft.tc) return fft.tc;
+        SW_CUDA(cudaStreamSynchronize(st));
+        for (auto& e : step_exec)
+            if (e) {
+                SW_CUDA(cudaGraphExecDestroy(e));
+                e = nullptr;
+            }
+        return fft.set_tile(columns);
+    }
+
     // Autotuner of the 2-D transform launches: times `reps` forward + inverse
-    // transforms of the pressure sweep's batch (3*nz planes per member) at each
-    // candidate chunk (cap, cap/2, ... down to 8 planes) with CUDA events on the
-    // context's stream, and keeps the fastest.  The batch runs on scratch buffers
-    // allocated for the measurement.  Writes up to maxc (chunk, ms per transform
-    // pair) rows and returns the chosen chunk.
-    int autotune_fft(int reps, int maxc, int* cand, float* ms, int* ncand) {
+    // transforms of the pressure sweep's batch (3*nz planes per member) for each
+    // tile width the length has compiled kernels for (n = 256: 16 and 32 columns)
+    // and each chunk (cap, cap/2, ... down to 8 planes), with CUDA events on the
+    // context's stream, and keeps the fastest pair.  The batch runs on scratch
+    // buffers allocated for the measurement.  Writes up to maxc (tile, chunk, ms
+    // per transform pair) rows; returns the chosen chunk and sets *tile_out.
+    int autotune_fft(int reps, int maxc, int* tiles, int* cand, float* ms, int* ncand, int* tile_out) {
         if (reps < 1) reps = 1;
         const int nb = std::min(fft.cap, 3 * nz * M);
         DevBuf<T> a, b;
@@ -538,36 +552,43 @@ struct Solver {
         cudaEvent_t e0, e1;
         SW_CUDA(cudaEventCreate(&e0));
         SW_CUDA(cudaEventCreate(&e1));
-        std::vector<int> cands;
+        std::vector<int> cands, tcs;
         for (int c = fft.cap;; c /= 2) {
             cands.push_back(c);
             if (c / 2 < 8) break;
         }
-        int best = fft.chunk, k = 0;
+        if (ng == FFT_R_N) tcs = {16, 32};
+        else tcs = {fft.tc};
+        int best = fft.chunk, best_tc = fft.tc, k = 0;
         float best_ms = 1e30f;
         try {
-            for (int c : cands) {
-                set_fft_chunk(c);
-                for (int r = -1; r < reps; r++) {  // r = -1: untimed warm-up
-                    if (r == 0) SW_CUDA(cudaEventRecord(e0, st));
-                    fft.ptospc(st, nb, [=] __device__(int o, int iy, int ix) -> T { return A[((size_t)o * ng + ix) * ng + iy]; },
-                               [=] __device__(int o, int kx, int ky, T v) { B[((size_t)o * ng + ky) * ng + kx] = v; });
-                    fft.spctop(st, nb, [=] __device__(int o, int kx, int ky) -> T { return B[((size_t)o * ng + ky) * ng + kx]; },
-                               [=] __device__(int o, int iy, int ix, T v) { A[((size_t)o * ng + ix) * ng + iy] = v; });
-                }
-                SW_CUDA(cudaEventRecord(e1, st));
-                SW_CUDA(cudaEventSynchronize(e1));
-                float t = 0.f;
-                SW_CUDA(cudaEventElapsedTime(&t, e0, e1));
-                t /= (float)(reps > 0 ? reps : 1);
-                if (k < maxc) {
-                    if (cand) cand[k] = fft.chunk;
-                    if (ms) ms[k] = t;
-                }
-                k++;
-                if (t < best_ms) {
-                    best_ms = t;
-                    best = fft.chunk;
+            for (int tcv : tcs) {
+                set_fft_tile(tcv);
+                for (int c : cands) {
+                    set_fft_chunk(c);
+                    for (int r = -1; r < reps; r++) {  // r = -1: untimed warm-up
+                        if (r == 0) SW_CUDA(cudaEventRecord(e0, st));
+                        fft.ptospc(st, nb, [=] __device__(int o, int iy, int ix) -> T { return A[((size_t)o * ng + ix) * ng + iy]; },
+                                   [=] __device__(int o, int kx, int ky, T v) { B[((size_t)o * ng + ky) * ng + kx] = v; });
+                        fft.spctop(st, nb, [=] __device__(int o, int kx, int ky) -> T { return B[((size_t)o * ng + ky) * ng + kx]; },
+                                   [=] __device__(int o, int iy, int ix, T v) { A[((size_t)o * ng + ix) * ng + iy] = v; });
+                    }
+                    SW_CUDA(cudaEventRecord(e1, st));
+                    SW_CUDA(cudaEventSynchronize(e1));
+                    float t = 0.f;
+                    SW_CUDA(cudaEventElapsedTime(&t, e0, e1));
+                    t /= (float)reps;
+                    if (k < maxc) {
+                        if (tiles) tiles[k] = fft.tc;
+                        if (cand) cand[k] = fft.chunk;
+                        if (ms) ms[k] = t;
+                    }
+                    k++;
+                    if (t < best_ms) {
+                        best_ms = t;
+                        best = fft.chunk;
+                        best_tc = fft.tc;
+                    }
                 }
             }
         } catch (...) {
@@ -578,6 +599,8 @@ struct Solver {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (ncand) *ncand = k < maxc ? k : maxc;
+        const int tc_set = set_fft_tile(best_tc);
+        if (tile_out) *tile_out = tc_set;
         return set_fft_chunk(best);
     }
 

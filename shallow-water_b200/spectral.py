@@ -65,14 +65,25 @@ class Spectral:
         check(lib().sw_set_fft_chunk(self._ctx, int(planes), ctypes.byref(v)))
         return v.value
 
-    def autotune(self, reps=5, maxc=16):
-        """Time the candidate transform chunks on this context's grid and keep the
-        fastest.  Returns {"chosen": planes, "candidates": [(planes, ms), ...]}."""
+    def set_fft_tile(self, columns):
+        """Columns per tile of the n = 256 passes (16 or 32; <= 0 only queries);
+        returns the value in use."""
+        v = ctypes.c_int()
+        check(lib().sw_set_fft_tile(self._ctx, int(columns), ctypes.byref(v)))
+        return v.value
+
+    def autotune(self, reps=5, maxc=32):
+        """Time the candidate tile widths and transform chunks on this context's
+        grid and keep the fastest.  Returns {"tile": columns, "chosen": planes,
+        "candidates": [(columns, planes, ms), ...]}."""
+        tiles = (ctypes.c_int * maxc)()
         chunks = (ctypes.c_int * maxc)()
         ms = (ctypes.c_float * maxc)()
-        n, chosen = ctypes.c_int(), ctypes.c_int()
-        check(lib().sw_autotune_fft(self._ctx, int(reps), maxc, chunks, ms, ctypes.byref(n), ctypes.byref(chosen)))
-        return {"chosen": chosen.value, "candidates": [(chunks[i], float(ms[i])) for i in range(n.value)]}
+        n, tile, chosen = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().sw_autotune_fft(self._ctx, int(reps), maxc, tiles, chunks, ms, ctypes.byref(n),
+                                    ctypes.byref(tile), ctypes.byref(chosen)))
+        return {"tile": tile.value, "chosen": chosen.value,
+                "candidates": [(tiles[i], chunks[i], float(ms[i])) for i in range(n.value)]}
 
     @property
     def n2(self):

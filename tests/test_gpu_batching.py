@@ -52,7 +52,8 @@ def test_float32_transform_256_vs_oracle(sw, oracle):
 
 @pytest.mark.parametrize("precision,ng", [(p, n) for p in ("fp64", "mixed") for n in (64, 256)])
 def test_transform_chunk_does_not_change_results(sw, precision, ng):
-    """Planes per launch pair only changes the launch shape: bit-identical output."""
+    """Planes per launch pair and (at n = 256) columns per tile only change the
+    launch shape: bit-identical output."""
     prec = sw.SW_FP64 if precision == "fp64" else sw.SW_MIXED
     dtype = np.float64 if precision == "fp64" else np.float32
     nz = 4
@@ -60,10 +61,13 @@ def test_transform_chunk_does_not_change_results(sw, precision, ng):
     rng = np.random.default_rng(5)
     x = rng.standard_normal(40 * ng * ng)
     outs = []
-    for chunk in (1, 7, 10 ** 6):
-        used = sp.set_fft_chunk(chunk)
-        assert used >= 1
-        outs.append((_fft2d(sw, sp, 0, x, dtype), _fft2d(sw, sp, 1, x, dtype)))
+    for tile in ((16, 32) if ng == 256 else (0,)):
+        if tile:
+            assert sp.set_fft_tile(tile) == tile
+        for chunk in (1, 7, 10 ** 6):
+            used = sp.set_fft_chunk(chunk)
+            assert used >= 1
+            outs.append((_fft2d(sw, sp, 0, x, dtype), _fft2d(sw, sp, 1, x, dtype)))
     for o in outs[1:]:
         assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
 
@@ -106,8 +110,8 @@ def test_autotune_reports_candidates_and_keeps_results(sw):
         sp = _ensemble(sw, ng, nz, M, sw.SW_FP64, 40)
         if tune:
             rep = sp.autotune(reps=2)
-            assert rep["candidates"] and rep["chosen"] in [c for c, _ in rep["candidates"]]
-            assert all(ms > 0 for _, ms in rep["candidates"])
+            assert rep["candidates"] and (rep["tile"], rep["chosen"]) in [(t, c) for t, c, _ in rep["candidates"]]
+            assert all(ms > 0 for _, _, ms in rep["candidates"])
         sw._native.check(sw._native.lib().sw_advance(sp.ctx, 2, 1))
         runs.append(_fields(sw, sp, M))
     for m in range(M):
