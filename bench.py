@@ -239,7 +239,8 @@ def fft_only(sw, sp, args, w_fft):
     per, nbytes = time_fft_pass(sw, sp, args.planes, w_fft, reps=args.steps)
     peak, kind = measured_peak()
     print(json.dumps({"fft_pass_us": per * 1e6, "bytes_per_launch": nbytes, "gbs": nbytes / per / 1e9,
-                      "frac": nbytes / per / 1e9 / peak, "planes": args.planes, "precision": args.precision}))
+                      "frac": nbytes / per / 1e9 / peak, "planes": args.planes, "precision": args.precision,
+                      "tile": sp.set_fft_tile(0)}))
     return 0
 
 
@@ -620,6 +621,8 @@ def main():
     ap.add_argument("--fft-only", action="store_true",
                     help="only time the batched 2-D transform pass (for profiling the top kernel)")
     ap.add_argument("--planes", type=int, default=None, help="planes of the --fft-only pass (default 6*(nz+1))")
+    ap.add_argument("--fft-tile", type=int, default=0, choices=[0, 16, 32],
+                    help="columns per tile of the --fft-only pass at ng=256 (0: the precision's default)")
     ap.add_argument("--ng", type=int, default=NG, help="horizontal grid (the headline workload is 256)")
     ap.add_argument("--nz", type=int, default=NZ, help="layers (the headline workload is 16)")
     ap.add_argument("--kernels", action="store_true",
@@ -661,7 +664,11 @@ def main():
     sw = load_package()
     if args.fft_only:
         prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
-        sp = sw.Spectral(NG, NZ, precision=prec, nmembers=1, device=local)
+        # the intermediate holds 6 (nz+1) planes per member: enough members for --planes
+        nmem = max(1, -(-args.planes // (6 * (NZ + 1))))
+        sp = sw.Spectral(NG, NZ, precision=prec, nmembers=nmem, device=local)
+        if args.fft_tile:
+            sp.set_fft_tile(args.fft_tile)
         return fft_only(sw, sp, args, 8 if prec == sw.SW_FP64 else 4)
     if args.kernels:
         return kernels(sw, args, rank, local)

@@ -680,15 +680,21 @@ struct Solver {
                 rv.v[1] = (double)V[p] * (double)R[p];
                 return rv;
             }, red_partial.p, sums);
+        // (uio, vio) per member once, after the per-plane sums (not per element)
         const double dsumi = 1.0 / (double)(ng * ng);
-        for_planes(st, ML, n2, [=] __device__(int q, int i) {
-            const int m = q / L;
+        double* mean = sums + 2 * ML;
+        for_cols(st, M, [=] __device__(int m) {
             double uio = 0.0, vio = 0.0;
-            #pragma unroll 4
             for (int iz = 0; iz < L; iz++) {
                 uio -= wgt[iz] * sums[2 * (m * L + iz)] * dsumi;
                 vio -= wgt[iz] * sums[2 * (m * L + iz) + 1] * dsumi;
             }
+            mean[2 * m] = uio;
+            mean[2 * m + 1] = vio;
+        });
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L;
+            const double uio = mean[2 * m], vio = mean[2 * m + 1];
             const size_t p = (size_t)q * n2 + i;
             U[p] = (T)((double)U[p] + uio);
             V[p] = (T)((double)V[p] + vio);
@@ -1507,44 +1513,48 @@ struct Solver {
             launch_pass<T, true, true, true>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, 3 * nz * mc, ng,
                 SweepMidLoad<T>{fft.mid.p, ng, nz}, SweepPhysStore<T>{A, B, C, ng, nz, L, m0});
         }
-        // (b) total source S = S0 + S1(p), to spectral space
+        // (b) total source S = S0 + S1(p) in physical space, then to spectral space.
+        //     S reads eight fields per element; as a streaming pass at full occupancy
+        //     it runs near the memory bandwidth, while inside the transform's loader
+        //     (sixteen pairs per thread, four CTAs per SM) the loads wait on latency.
+        T* SRC = D;
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L, iz = q % L;
+            const size_t p = (size_t)q * n2 + i;
+            const size_t cb = (size_t)m * L * n2 + i;
+            auto P = [&](int l) { return l >= nz ? 0.0 : (double)A[cb + (size_t)l * n2]; };
+            auto X = [&](int l) { return l >= nz ? 0.0 : (double)B[cb + (size_t)l * n2]; };
+            auto Y = [&](int l) { return l >= nz ? 0.0 : (double)C[cb + (size_t)l * n2]; };
+            double s;
+            if (iz == 0) {
+                const double d2 = (2.0 * P(0) - 5.0 * P(1) + 4.0 * P(2) - P(3)) * dzisq;
+                s = (double)SP0[p] + (double)C2[p] * d2;
+            } else if (iz < nz) {
+                const double dxt = (X(iz + 1) - X(iz - 1)) * hdzi;
+                const double dyt = (Y(iz + 1) - Y(iz - 1)) * hdzi;
+                const double dpdt = (P(iz + 1) - P(iz - 1)) * hdzi;
+                const double d2 = (P(iz + 1) - 2.0 * P(iz) + P(iz - 1)) * dzisq;
+                s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
+                s += (double)C2[p] * d2 + (double)C1[p] * dpdt;
+            } else {
+                // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238)
+                auto ext = [&](auto F) {
+                    const double a1 = (F(nz) - F(nz - 2)) * hdzi;
+                    const double d1 = (F(nz) - 2.0 * F(nz - 1) + F(nz - 2)) * dzisq;
+                    const double d2 = (F(nz - 1) - 2.0 * F(nz - 2) + F(nz - 3)) * dzisq;
+                    return a1 + dz2 * (3.0 * d1 - d2);
+                };
+                const double dxt = ext(X), dyt = ext(Y), dpdt = ext(P);
+                const double d1 = (P(nz) - 2.0 * P(nz - 1) + P(nz - 2)) * dzisq;
+                const double d2 = (P(nz - 1) - 2.0 * P(nz - 2) + P(nz - 3)) * dzisq;
+                const double d2pdt2 = 2.0 * d1 - d2;
+                s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
+                s += (double)C2[p] * d2pdt2 + (double)C1[p] * dpdt;
+            }
+            SRC[p] = (T)s;
+        });
         fft.ptospc(st, ML,
-            [=] __device__(int q, int iy, int ix) -> T {
-                const int m = q / L, iz = q % L;
-                const int i = iy + ng * ix;
-                const size_t p = (size_t)q * n2 + i;
-                const size_t cb = (size_t)m * L * n2 + i;
-                auto P = [&](int l) { return l >= nz ? 0.0 : (double)A[cb + (size_t)l * n2]; };
-                auto X = [&](int l) { return l >= nz ? 0.0 : (double)B[cb + (size_t)l * n2]; };
-                auto Y = [&](int l) { return l >= nz ? 0.0 : (double)C[cb + (size_t)l * n2]; };
-                double s;
-                if (iz == 0) {
-                    const double d2 = (2.0 * P(0) - 5.0 * P(1) + 4.0 * P(2) - P(3)) * dzisq;
-                    s = (double)SP0[p] + (double)C2[p] * d2;
-                } else if (iz < nz) {
-                    const double dxt = (X(iz + 1) - X(iz - 1)) * hdzi;
-                    const double dyt = (Y(iz + 1) - Y(iz - 1)) * hdzi;
-                    const double dpdt = (P(iz + 1) - P(iz - 1)) * hdzi;
-                    const double d2 = (P(iz + 1) - 2.0 * P(iz) + P(iz - 1)) * dzisq;
-                    s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
-                    s += (double)C2[p] * d2 + (double)C1[p] * dpdt;
-                } else {
-                    // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238)
-                    auto ext = [&](auto F) {
-                        const double a1 = (F(nz) - F(nz - 2)) * hdzi;
-                        const double d1 = (F(nz) - 2.0 * F(nz - 1) + F(nz - 2)) * dzisq;
-                        const double d2 = (F(nz - 1) - 2.0 * F(nz - 2) + F(nz - 3)) * dzisq;
-                        return a1 + dz2 * (3.0 * d1 - d2);
-                    };
-                    const double dxt = ext(X), dyt = ext(Y), dpdt = ext(P);
-                    const double d1 = (P(nz) - 2.0 * P(nz - 1) + P(nz - 2)) * dzisq;
-                    const double d2 = (P(nz - 1) - 2.0 * P(nz - 2) + P(nz - 3)) * dzisq;
-                    const double d2pdt2 = 2.0 * d1 - d2;
-                    s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
-                    s += (double)C2[p] * d2pdt2 + (double)C1[p] * dpdt;
-                }
-                return (T)s;
-            },
+            [=] __device__(int q, int iy, int ix) -> T { return SRC[(size_t)q * n2 + iy + ng * ix]; },
             [=] __device__(int q, int kx, int ky, T val) { SP[(size_t)q * n2 + kx + ng * ky] = val; });
         // (c) compact RHS and Thomas solve per (kx, ky) column, with the errp sums
         //     reduced per CTA; (d) one control kernel finishes the sums per member and
