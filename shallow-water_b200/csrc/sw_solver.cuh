@@ -1360,24 +1360,34 @@ struct Solver {
                 const int k = o - 3 * Mnz - 2 * ML, m = k / nz, iz = 1 + k % nz;
                 D[(size_t)(m * L + iz) * n2 + pi] = val;
             });
-        // P6: cpt2's argument and cpsource's dealiased products
-        // (level-major: the four outputs of one level are adjacent planes, so the
-        // fields they share are read from L2)
+        // P6: cpt2's argument and cpsource's dealiased products.  The four values of
+        // an element share the theta derivatives of u, v, w: one streaming pass forms
+        // them into staging planes (W(8), W(9), W(10), W(17): consumed by P2 and P5),
+        // then a plain transform takes them to spectral space.
+        T *G0 = W(8), *G1 = W(9), *G2 = W(10), *G3 = W(17);
+        for_planes(st, ML, n2, [=] __device__(int q, int pi) {
+            const int m = q / L, iz = q % L;
+            const size_t p = (size_t)q * n2 + pi;
+            G0[p] = T(1) - RI[p] * RI[p] - SIGX[p] * SIGX[p] - SIGY[p] * SIGY[p];
+            const size_t cb = (size_t)m * L * n2 + pi;
+            const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
+            if (iz == 0) {
+                G1[p] = T(0);
+                G2[p] = (T)((double)RI[p] * wt);
+                G3[p] = T(0);
+                return;
+            }
+            const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
+            const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
+            G1[p] = (T)(vt * (double)ZX[p] - ut * (double)ZY[p]);
+            G2[p] = (T)((double)UY[p] * vt - ut * (double)VY[p]);
+            G3[p] = (T)(ut * (double)VX[p] - (double)UX[p] * vt);
+        });
         fft.ptospc(st, 4 * ML,
             [=] __device__(int o, int iy, int ix) -> T {
-                const int which = o & 3, q = o >> 2, m = q / L, iz = q % L;
-                const int pi = iy + ng * ix;
-                const size_t p = (size_t)q * n2 + pi;
-                if (which == 0) return T(1) - RI[p] * RI[p] - SIGX[p] * SIGX[p] - SIGY[p] * SIGY[p];
-                const size_t cb = (size_t)m * L * n2 + pi;
-                const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
-                if (which == 2 && iz == 0) return (T)((double)RI[p] * wt);
-                if (iz == 0) return T(0);
-                const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
-                const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
-                if (which == 1) return (T)(vt * (double)ZX[p] - ut * (double)ZY[p]);
-                if (which == 2) return (T)((double)UY[p] * vt - ut * (double)VY[p]);
-                return (T)(ut * (double)VX[p] - (double)UX[p] * vt);
+                const int which = o & 3, q = o >> 2;
+                const T* g = which == 0 ? G0 : which == 1 ? G1 : which == 2 ? G2 : G3;
+                return g[(size_t)q * n2 + iy + ng * ix];
             },
             [=] __device__(int o, int kx, int ky, T val) {
                 const int which = o & 3, q = o >> 2, i = kx + ng * ky;
@@ -1413,55 +1423,61 @@ struct Solver {
             SIGX[p] = SIGX[p] * T(2);
             SIGY[p] = SIGY[p] * T(2);
         });
-        // P9/P10: the second dealiased product and sp0 (cpsource.rs:222-258)
+        // P9/P10: the second dealiased product and sp0 (cpsource.rs:222-258), both
+        // formed in streaming passes around plain transforms (staging in W(8), W(9))
+        T *G = W(8), *Gq = W(9);
+        for_planes(st, ML, n2, [=] __device__(int q, int pi) {
+            const int m = q / L, iz = q % L;
+            const size_t p = (size_t)q * n2 + pi;
+            if (iz == 0) {
+                G[p] = T(0);
+                return;
+            }
+            const size_t cb = (size_t)m * L * n2 + pi;
+            const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
+            const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
+            const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
+            double wkq = (double)Pq[p] * (double)ZX[p] + (double)Pr[p] * (double)ZY[p] - (double)WY[p] * vt;
+            wkq += ((double)UX[p] + (double)VY[p]) * wt - (double)WX[p] * ut;
+            G[p] = (T)wkq;
+        });
         fft.ptospc(st, ML,
-            [=] __device__(int q, int iy, int ix) -> T {
-                const int m = q / L, iz = q % L;
-                if (iz == 0) return T(0);
-                const int pi = iy + ng * ix;
-                const size_t p = (size_t)q * n2 + pi;
-                const size_t cb = (size_t)m * L * n2 + pi;
-                const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
-                const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
-                const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
-                double wkq = (double)Pq[p] * (double)ZX[p] + (double)Pr[p] * (double)ZY[p] - (double)WY[p] * vt;
-                wkq += ((double)UX[p] + (double)VY[p]) * wt - (double)WX[p] * ut;
-                return (T)wkq;
-            },
+            [=] __device__(int q, int iy, int ix) -> T { return G[(size_t)q * n2 + iy + ng * ix]; },
             [=] __device__(int q, int kx, int ky, T val) {
                 const int i = kx + ng * ky;
                 Sq2[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
             });
         fft.spctop(st, ML,
             [=] __device__(int q, int kx, int ky) -> T { return Sq2[(size_t)q * n2 + kx + ng * ky]; },
-            [=] __device__(int q, int iy, int ix, T val) {
-                const int m = q / L, iz = q % L;
-                const int pi = iy + ng * ix;
-                const size_t p = (size_t)q * n2 + pi;
-                const double ux = UX[p], uy = UY[p], vx = VX[p], vy = VY[p];
-                double s;
-                if (mixed) {
-                    const double hz = HZ[p];
-                    if (iz == 0) {
-                        s = hz + 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
-                    } else {
-                        const double rip = RI[p];
-                        s = hz - COF * (rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
-                        s += 2.0 * (ux * vy - uy * vx);
-                    }
+            [=] __device__(int q, int iy, int ix, T val) { Gq[(size_t)q * n2 + iy + ng * ix] = val; });
+        for_planes(st, ML, n2, [=] __device__(int q, int pi) {
+            const int m = q / L, iz = q % L;
+            const size_t p = (size_t)q * n2 + pi;
+            const T val = Gq[p];
+            const double ux = UX[p], uy = UY[p], vx = VX[p], vy = VY[p];
+            double s;
+            if (mixed) {
+                const double hz = HZ[p];
+                if (iz == 0) {
+                    s = hz + 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
                 } else {
-                    const double hsv = (double)hsrc[(size_t)m * n2 + pi];
-                    if (iz == 0) {
-                        s = hsv + COF * (double)ZE[p];
-                        s += 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
-                    } else {
-                        const double rip = RI[p];
-                        s = hsv + COF * ((double)ZE[p] - rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
-                        s += 2.0 * (ux * vy - uy * vx);
-                    }
+                    const double rip = RI[p];
+                    s = hz - COF * (rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
+                    s += 2.0 * (ux * vy - uy * vx);
                 }
-                SP0[p] = (T)s;
-            });
+            } else {
+                const double hsv = (double)hsrc[(size_t)m * n2 + pi];
+                if (iz == 0) {
+                    s = hsv + COF * (double)ZE[p];
+                    s += 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
+                } else {
+                    const double rip = RI[p];
+                    s = hsv + COF * ((double)ZE[p] - rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
+                    s += 2.0 * (ux * vy - uy * vx);
+                }
+            }
+            SP0[p] = (T)s;
+        });
         int* ctl = ctrl.p;
         for_cols(st, M, [=] __device__(int m) {
             ctl[3 * m] = 1;
