@@ -641,29 +641,31 @@ struct Solver {
         });
         T *R = r, *U = u, *V = v, *ZE = zeta;
         T *SU = W(8), *SV = W(9);  // spectral u, v for psolve's set-up in this stage
-        // level-major: r, zeta, u, v of one level are adjacent planes, so qs, ds, gs
-        // are read from DRAM once and from L2 by the other three
+        // spectral r and zeta staged in W(10), W(17) (written by P5 and source
+        // before any read there): one streaming pass forms the four spectral inputs
+        // of an element, then a plain transform takes them to physical space
+        T *SR = W(10), *SZ = W(17);
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L;
+            const int kx = i % ng, ky = i / ng;
+            const double* qsq = QS + (size_t)q * n2;
+            const double* dsq = DS + (size_t)q * n2;
+            const double* gsq = GS + (size_t)q * n2;
+            const double* wk = wkh + (size_t)m * n2;
+            auto wka = [&](int j) { return COFI * (COFI * gsq[j] - qsq[j]) - wk[j]; };
+            auto wkb = [&](int j) { return qsq[j] + COF * wka(j); };
+            const size_t p = (size_t)q * n2 + i;
+            SR[p] = (T)wka(i);
+            SZ[p] = (T)wkb(i);
+            const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+            SU[p] = (T)(dmul(kx, ng) * (rlap[mx] * dsq[mx]) - dmul(ky, ng) * (rlap[my] * wkb(my)));
+            SV[p] = (T)(dmul(ky, ng) * (rlap[my] * dsq[my]) + dmul(kx, ng) * (rlap[mx] * wkb(mx)));
+        });
         fft.spctop(st, 4 * ML,
             [=] __device__(int o, int kx, int ky) -> T {
-                const int which = o & 3, q = o >> 2, m = q / L;
-                const double* qsq = QS + (size_t)q * n2;
-                const double* dsq = DS + (size_t)q * n2;
-                const double* gsq = GS + (size_t)q * n2;
-                const double* wk = wkh + (size_t)m * n2;
-                auto wka = [&](int i) { return COFI * (COFI * gsq[i] - qsq[i]) - wk[i]; };
-                auto wkb = [&](int i) { return qsq[i] + COF * wka(i); };
-                const int i = kx + ng * ky;
-                if (which == 0) return (T)wka(i);
-                if (which == 1) return (T)wkb(i);
-                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
-                if (which == 2) {
-                    const T val = (T)(dmul(kx, ng) * (rlap[mx] * dsq[mx]) - dmul(ky, ng) * (rlap[my] * wkb(my)));
-                    SU[(size_t)q * n2 + i] = val;
-                    return val;
-                }
-                const T val = (T)(dmul(ky, ng) * (rlap[my] * dsq[my]) + dmul(kx, ng) * (rlap[mx] * wkb(mx)));
-                SV[(size_t)q * n2 + i] = val;
-                return val;
+                const int which = o & 3, q = o >> 2;
+                const T* g = which == 0 ? SR : which == 1 ? SZ : which == 2 ? SU : SV;
+                return g[(size_t)q * n2 + kx + ng * ky];
             },
             [=] __device__(int o, int iy, int ix, T val) {
                 const int which = o & 3, q = o >> 2;
@@ -1817,27 +1819,29 @@ struct Solver {
                        : which == 5 ? UX : which == 6 ? UY : which == 7 ? VX : VY;
                 out[(size_t)q * n2 + i] = val;
             });
-        // products to spectral space
-        fft.ptospc(st, 6 * ML,  // level-major (outputs sharing inputs are adjacent planes)
+        // products to spectral space: the six products of an element are formed in
+        // one streaming pass into staging planes (W(0..4), W(7): the pressure
+        // sweep's work planes and F, all consumed by now), then transformed
+        T *G0 = W(0), *G1 = W(1), *G2 = W(2), *G3 = W(3), *G4 = W(4), *G5 = W(7);
+        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L, iz = q % L;
+            const size_t p = (size_t)q * n2 + i;
+            const T u = U[p], v = V[p], zx = ZX[p], zy = ZY[p], ff = FF[p], dd = DD[p];
+            const T qv = q_phys ? (T)((double)ZE[p] - COF * (double)R[p]) : Q[p];
+            G0[p] = qv * u;
+            G1[p] = qv * v;
+            const T bx = iz == 0 ? zx0[(size_t)m * n2 + i] : zx;
+            const T by = iz == 0 ? zy0[(size_t)m * n2 + i] : zy;
+            G2[p] = FX[p] * by - FY[p] * bx;
+            G3[p] = UX[p] * VY[p] - UY[p] * VX[p];
+            G4[p] = ff * zx - dd * u;
+            G5[p] = ff * zy - dd * v;
+        });
+        fft.ptospc(st, 6 * ML,  // level-major
             [=] __device__(int o, int iy, int ix) -> T {
-                const int q = o / 6, which = o - 6 * q, m = q / L, iz = q % L;
-                const int i = iy + ng * ix;
-                const size_t p = (size_t)q * n2 + i;
-                switch (which) {
-                    case 0:
-                    case 1: {
-                        const T qv = q_phys ? (T)((double)ZE[p] - COF * (double)R[p]) : Q[p];
-                        return qv * (which == 0 ? U[p] : V[p]);
-                    }
-                    case 2: {
-                        const T bx = iz == 0 ? zx0[(size_t)m * n2 + i] : ZX[p];
-                        const T by = iz == 0 ? zy0[(size_t)m * n2 + i] : ZY[p];
-                        return FX[p] * by - FY[p] * bx;
-                    }
-                    case 3: return UX[p] * VY[p] - UY[p] * VX[p];
-                    case 4: return FF[p] * ZX[p] - DD[p] * U[p];
-                    default: return FF[p] * ZY[p] - DD[p] * V[p];
-                }
+                const int q = o / 6, which = o - 6 * q;
+                const T* g = which == 0 ? G0 : which == 1 ? G1 : which == 2 ? G2 : which == 3 ? G3 : which == 4 ? G4 : G5;
+                return g[(size_t)q * n2 + iy + ng * ix];
             },
             [=] __device__(int o, int kx, int ky, T val) {
                 const int q = o / 6, which = o - 6 * q;
