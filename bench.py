@@ -31,11 +31,13 @@ NG, NZ = 256, 16
 METRIC = "member-steps/s at ng=256 nz=16"
 UNIT = "member-steps/s"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, ncu) of one tile pass
-# over 102 planes at ng=256, averaged over the two forward and two reverse passes
-# of the transform micro-benchmark.  Reads are the plane data; the written planes
-# mostly stay in the 126 MB L2 until after the kernel, so little write traffic is
-# attributed to the pass itself.
-FFT_PASS_DRAM_BYTES = {"mixed": 26.86e6, "fp64": 60.4e6}
+# at ng=256 by (precision, planes per launch), averaged over two forward and two
+# reverse passes of the transform micro-benchmark.  Reads are the plane data.  At
+# 102 planes the written planes mostly stay in the 126 MB L2 until after the
+# kernel; at 816 and 1632 planes most of them reach DRAM within it.
+FFT_PASS_DRAM_BYTES = {("mixed", 102): 26.86e6, ("fp64", 102): 60.4e6,
+                       ("mixed", 816): 377.7e6, ("mixed", 1632): 805.9e6,
+                       ("fp64", 816): 803.5e6, ("fp64", 1632): 1658.8e6}
 
 
 def load_package():
@@ -256,12 +258,16 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     M = args.members
     sp = sw.Spectral(NG, NZ, precision=prec, nmembers=M, device=local)
     sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
-    fft_pre = None
-    if full:  # the top kernel's pass (102 planes, one launch), timed on this context's stream
+    fft_pre = fft_step = None
+    if full:  # the top kernel's pass over one member's 102 planes, timed on this context's stream
         chunk = sp.set_fft_chunk(0)
         fft_pre = time_fft_pass(sw, sp, 6 * (NZ + 1), w_fft)
         sp.set_fft_chunk(chunk)
     tune = sp.autotune() if args.autotune == "on" else None
+    if full:  # and at the planes per launch the step's batched transforms use (the chunk)
+        chunk = sp.set_fft_chunk(0)
+        fft_step = (chunk,) + time_fft_pass(sw, sp, chunk, w_fft)
+        sp.set_fft_chunk(chunk)
     qq2 = sw.vstrip.pv_strip(NG)
     for m in range(M):
         q3, d3, g3 = initial_fields(NG, NZ, args.seed0 + rank * M + m, lambda ng: qq2)
@@ -330,10 +336,8 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
             pipe = e2e_pipelined(sw, L, args, M, prec, local, rank, tune, e2e_steps, world, barrier)
             res["e2e_sequential"] = res["e2e"]
             res["e2e"] = pipe
-        planes = 6 * (NZ + 1)
-        per_launch_s, bytes_per_launch = time_fft_pass(sw, sp, planes, w_fft)
-        res["fft"] = {"planes": planes, "per_launch_s": fft_pre[0], "bytes": fft_pre[1],
-                      "per_launch_s_after_run": per_launch_s}
+        res["fft"] = {"planes": fft_step[0], "per_launch_s": fft_step[1], "bytes": fft_step[2],
+                      "one_member": {"planes": 6 * (NZ + 1), "per_launch_s": fft_pre[0], "bytes": fft_pre[1]}}
     sp.close()
     torch.cuda.synchronize()
     return res
@@ -687,8 +691,12 @@ def main():
     M = args.members
     w_fft = main_arm["w_fft"]
     peak, peak_kind = measured_peak()
-    achieved = main_arm["fft"]["bytes"] / main_arm["fft"]["per_launch_s"] / 1e9
-    traffic = FFT_PASS_DRAM_BYTES.get(args.precision) if (NG, NZ) == (256, 16) else None
+    fft = main_arm["fft"]
+    achieved = fft["bytes"] / fft["per_launch_s"] / 1e9
+    one = fft["one_member"]
+    achieved_one = one["bytes"] / one["per_launch_s"] / 1e9
+    traffic = FFT_PASS_DRAM_BYTES.get((args.precision, fft["planes"])) if NG == 256 else None
+    traffic_one = FFT_PASS_DRAM_BYTES.get((args.precision, one["planes"])) if NG == 256 else None
     step_bytes = algorithmic_bytes_per_step(NG, NZ, main_arm["sweeps"], w_fft)
     step_gbs = step_bytes * (args.steps * M / main_arm["t_local"]) / 1e9
 
@@ -713,10 +721,12 @@ def main():
             "e2e": main_arm["e2e"],
             "e2e_sequential": main_arm.get("e2e_sequential"),
             "gpu_launches": main_arm["launches"],
-            "roofline": {"bound": "hbm", "kernel": "k_fft_pass (batched 2-D transform pass, %d planes)"
-                                                   % main_arm["fft"]["planes"],
+            "roofline": {"bound": "hbm", "kernel": "k_fft_pass_r (batched 2-D transform pass, %d planes per "
+                                                   "launch: the step's chunk)" % fft["planes"],
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
+                         "one_member_pass": {"planes": one["planes"], "achieved": achieved_one,
+                                             "frac": achieved_one / peak, "traffic": traffic_one},
                          "step_algorithmic_gbs": step_gbs, "step_frac": step_gbs / peak},
             "cpu_baseline": cpu,
             "clocks": main_arm["clocks"],
