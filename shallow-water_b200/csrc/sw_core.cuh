@@ -105,6 +105,41 @@ inline void for_planes(cudaStream_t s, int nplanes, int n2, F f) {
     count_launch();
 }
 
+// f(o, i) for o < nplanes and i = 0, 4, 8, ... < n2 (n2 % 4 == 0): one thread per
+// four consecutive elements, for bodies that move them with ld4 / st4.
+template <class F>
+__global__ void k_planes4(int n4, F f) {
+    const int o = blockIdx.y;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) f(o, 4 * i);
+}
+template <class F>
+inline void for_planes4(cudaStream_t s, int nplanes, int n2, F f) {
+    if (nplanes <= 0) return;
+    const int threads = 256, n4 = n2 / 4;
+    int bx = (n4 + threads - 1) / threads;
+    if (bx > 1024) bx = 1024;
+    dim3 grid(bx, nplanes);
+    k_planes4<<<grid, threads, 0, s>>>(n4, f);
+    SW_CHECK_LAUNCH();
+    count_launch();
+}
+// Four consecutive elements at p (p 16-byte aligned for float, 32 for double).
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
 // f(c) for c < ncols: one thread per (member, horizontal point) column.
 // Column bodies loop over levels; their loops are unrolled so that loads of
 // later levels are in flight while earlier ones are used.

@@ -1535,41 +1535,71 @@ struct Solver {
         //     S reads eight fields per element; as a streaming pass at full occupancy
         //     it runs near the memory bandwidth, while inside the transform's loader
         //     (sixteen pairs per thread, four CTAs per SM) the loads wait on latency.
+        // Four elements per thread with 16-byte loads and stores (n2 % 4 == 0: ng is even).
         T* SRC = D;
-        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+        for_planes4(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L, iz = q % L;
             const size_t p = (size_t)q * n2 + i;
             const size_t cb = (size_t)m * L * n2 + i;
-            auto P = [&](int l) { return l >= nz ? 0.0 : (double)A[cb + (size_t)l * n2]; };
-            auto X = [&](int l) { return l >= nz ? 0.0 : (double)B[cb + (size_t)l * n2]; };
-            auto Y = [&](int l) { return l >= nz ? 0.0 : (double)C[cb + (size_t)l * n2]; };
-            double s;
-            if (iz == 0) {
-                const double d2 = (2.0 * P(0) - 5.0 * P(1) + 4.0 * P(2) - P(3)) * dzisq;
-                s = (double)SP0[p] + (double)C2[p] * d2;
-            } else if (iz < nz) {
-                const double dxt = (X(iz + 1) - X(iz - 1)) * hdzi;
-                const double dyt = (Y(iz + 1) - Y(iz - 1)) * hdzi;
-                const double dpdt = (P(iz + 1) - P(iz - 1)) * hdzi;
-                const double d2 = (P(iz + 1) - 2.0 * P(iz) + P(iz - 1)) * dzisq;
-                s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
-                s += (double)C2[p] * d2 + (double)C1[p] * dpdt;
-            } else {
-                // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238)
-                auto ext = [&](auto F) {
-                    const double a1 = (F(nz) - F(nz - 2)) * hdzi;
-                    const double d1 = (F(nz) - 2.0 * F(nz - 1) + F(nz - 2)) * dzisq;
-                    const double d2 = (F(nz - 1) - 2.0 * F(nz - 2) + F(nz - 3)) * dzisq;
-                    return a1 + dz2 * (3.0 * d1 - d2);
+            T out[4];
+            if (iz > 0 && iz < nz) {
+                auto lv = [&](const T* f, int l, T(&v)[4]) {
+                    if (l >= nz) v[0] = v[1] = v[2] = v[3] = T(0);
+                    else ld4(f + cb + (size_t)l * n2, v);
                 };
-                const double dxt = ext(X), dyt = ext(Y), dpdt = ext(P);
-                const double d1 = (P(nz) - 2.0 * P(nz - 1) + P(nz - 2)) * dzisq;
-                const double d2 = (P(nz - 1) - 2.0 * P(nz - 2) + P(nz - 3)) * dzisq;
-                const double d2pdt2 = 2.0 * d1 - d2;
-                s = (double)SP0[p] + (double)SIGX[p] * dxt + (double)SIGY[p] * dyt;
-                s += (double)C2[p] * d2pdt2 + (double)C1[p] * dpdt;
+                T xp[4], xm[4], yp[4], ym[4], pp[4], pc[4], pm[4], sp0[4], sx[4], sy[4], c2[4], c1[4];
+                lv(B, iz + 1, xp);
+                lv(B, iz - 1, xm);
+                lv(C, iz + 1, yp);
+                lv(C, iz - 1, ym);
+                lv(A, iz + 1, pp);
+                lv(A, iz, pc);
+                lv(A, iz - 1, pm);
+                ld4(SP0 + p, sp0);
+                ld4(SIGX + p, sx);
+                ld4(SIGY + p, sy);
+                ld4(C2 + p, c2);
+                ld4(C1 + p, c1);
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const double dxt = ((double)xp[e] - (double)xm[e]) * hdzi;
+                    const double dyt = ((double)yp[e] - (double)ym[e]) * hdzi;
+                    const double dpdt = ((double)pp[e] - (double)pm[e]) * hdzi;
+                    const double d2 = ((double)pp[e] - 2.0 * (double)pc[e] + (double)pm[e]) * dzisq;
+                    double s = (double)sp0[e] + (double)sx[e] * dxt + (double)sy[e] * dyt;
+                    s += (double)c2[e] * d2 + (double)c1[e] * dpdt;
+                    out[e] = (T)s;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const size_t pe = p + e, ce = cb + e;
+                    auto P = [&](int l) { return l >= nz ? 0.0 : (double)A[ce + (size_t)l * n2]; };
+                    auto X = [&](int l) { return l >= nz ? 0.0 : (double)B[ce + (size_t)l * n2]; };
+                    auto Y = [&](int l) { return l >= nz ? 0.0 : (double)C[ce + (size_t)l * n2]; };
+                    double s;
+                    if (iz == 0) {
+                        const double d2 = (2.0 * P(0) - 5.0 * P(1) + 4.0 * P(2) - P(3)) * dzisq;
+                        s = (double)SP0[pe] + (double)C2[pe] * d2;
+                    } else {
+                        // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238)
+                        auto ext = [&](auto F) {
+                            const double a1 = (F(nz) - F(nz - 2)) * hdzi;
+                            const double d1 = (F(nz) - 2.0 * F(nz - 1) + F(nz - 2)) * dzisq;
+                            const double d2 = (F(nz - 1) - 2.0 * F(nz - 2) + F(nz - 3)) * dzisq;
+                            return a1 + dz2 * (3.0 * d1 - d2);
+                        };
+                        const double dxt = ext(X), dyt = ext(Y), dpdt = ext(P);
+                        const double d1 = (P(nz) - 2.0 * P(nz - 1) + P(nz - 2)) * dzisq;
+                        const double d2 = (P(nz - 1) - 2.0 * P(nz - 2) + P(nz - 3)) * dzisq;
+                        const double d2pdt2 = 2.0 * d1 - d2;
+                        s = (double)SP0[pe] + (double)SIGX[pe] * dxt + (double)SIGY[pe] * dyt;
+                        s += (double)C2[pe] * d2pdt2 + (double)C1[pe] * dpdt;
+                    }
+                    out[e] = (T)s;
+                }
             }
-            SRC[p] = (T)s;
+            st4(SRC + p, out);
         });
         fft.ptospc(st, ML,
             [=] __device__(int q, int iy, int ix) -> T { return SRC[(size_t)q * n2 + iy + ng * ix]; },
