@@ -896,6 +896,31 @@ struct Solver {
                            4.0 * (double)col[(size_t)(nz - 1) * n2]);
         return hdzi * ((double)col[(size_t)(iz + 1) * n2] - (double)col[(size_t)(iz - 1) * n2]);
     }
+    // tderiv of four consecutive columns (col 16-byte aligned for float, 32 for double)
+    static __device__ __forceinline__ void tderiv4(const T* col, int iz, int nz, int n2, double hdzi, double (&d)[4]) {
+        T a[4], b[4];
+        if (iz == 0 || iz == nz) {
+            T c[4];
+            if (iz == 0) {
+                ld4(col + n2, a);
+                ld4(col, b);
+                ld4(col + 2 * (size_t)n2, c);
+#pragma unroll
+                for (int e = 0; e < 4; e++) d[e] = hdzi * (4.0 * (double)a[e] - 3.0 * (double)b[e] - (double)c[e]);
+            } else {
+                ld4(col + (size_t)nz * n2, a);
+                ld4(col + (size_t)(nz - 2) * n2, b);
+                ld4(col + (size_t)(nz - 1) * n2, c);
+#pragma unroll
+                for (int e = 0; e < 4; e++) d[e] = hdzi * (3.0 * (double)a[e] + (double)b[e] - 4.0 * (double)c[e]);
+            }
+            return;
+        }
+        ld4(col + (size_t)(iz + 1) * n2, a);
+        ld4(col + (size_t)(iz - 1) * n2, b);
+#pragma unroll
+        for (int e = 0; e < 4; e++) d[e] = hdzi * ((double)a[e] - (double)b[e]);
+    }
 
     // ======================================================================
     // cpsource (src/nhswps/cpsource.rs:13-261): sp0
@@ -1366,24 +1391,49 @@ struct Solver {
         // an element share the theta derivatives of u, v, w: one streaming pass forms
         // them into staging planes (W(8), W(9), W(10), W(17): consumed by P2 and P5),
         // then a plain transform takes them to spectral space.
+        // (four elements per thread with 16-byte loads and stores; n2 % 4 == 0)
         T *G0 = W(8), *G1 = W(9), *G2 = W(10), *G3 = W(17);
-        for_planes(st, ML, n2, [=] __device__(int q, int pi) {
+        for_planes4(st, ML, n2, [=] __device__(int q, int pi) {
             const int m = q / L, iz = q % L;
             const size_t p = (size_t)q * n2 + pi;
-            G0[p] = T(1) - RI[p] * RI[p] - SIGX[p] * SIGX[p] - SIGY[p] * SIGY[p];
             const size_t cb = (size_t)m * L * n2 + pi;
-            const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
+            T ri[4], sx[4], sy[4], g0[4], g1[4], g2[4], g3[4];
+            ld4(RI + p, ri);
+            ld4(SIGX + p, sx);
+            ld4(SIGY + p, sy);
+#pragma unroll
+            for (int e = 0; e < 4; e++) g0[e] = T(1) - ri[e] * ri[e] - sx[e] * sx[e] - sy[e] * sy[e];
+            double wt[4];
+            tderiv4(WW + cb, iz, nz, n2, hdzi, wt);
             if (iz == 0) {
-                G1[p] = T(0);
-                G2[p] = (T)((double)RI[p] * wt);
-                G3[p] = T(0);
-                return;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    g1[e] = T(0);
+                    g2[e] = (T)((double)ri[e] * wt[e]);
+                    g3[e] = T(0);
+                }
+            } else {
+                double ut[4], vt[4];
+                tderiv4(U + cb, iz, nz, n2, hdzi, ut);
+                tderiv4(V + cb, iz, nz, n2, hdzi, vt);
+                T zx[4], zy[4], ux[4], uy[4], vx[4], vy[4];
+                ld4(ZX + p, zx);
+                ld4(ZY + p, zy);
+                ld4(UX + p, ux);
+                ld4(UY + p, uy);
+                ld4(VX + p, vx);
+                ld4(VY + p, vy);
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    g1[e] = (T)(vt[e] * (double)zx[e] - ut[e] * (double)zy[e]);
+                    g2[e] = (T)((double)uy[e] * vt[e] - ut[e] * (double)vy[e]);
+                    g3[e] = (T)(ut[e] * (double)vx[e] - (double)ux[e] * vt[e]);
+                }
             }
-            const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
-            const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
-            G1[p] = (T)(vt * (double)ZX[p] - ut * (double)ZY[p]);
-            G2[p] = (T)((double)UY[p] * vt - ut * (double)VY[p]);
-            G3[p] = (T)(ut * (double)VX[p] - (double)UX[p] * vt);
+            st4(G0 + p, g0);
+            st4(G1 + p, g1);
+            st4(G2 + p, g2);
+            st4(G3 + p, g3);
         });
         fft.ptospc(st, 4 * ML,
             [=] __device__(int o, int iy, int ix) -> T {
@@ -1428,20 +1478,36 @@ struct Solver {
         // P9/P10: the second dealiased product and sp0 (cpsource.rs:222-258), both
         // formed in streaming passes around plain transforms (staging in W(8), W(9))
         T *G = W(8), *Gq = W(9);
-        for_planes(st, ML, n2, [=] __device__(int q, int pi) {
+        for_planes4(st, ML, n2, [=] __device__(int q, int pi) {
             const int m = q / L, iz = q % L;
             const size_t p = (size_t)q * n2 + pi;
+            T g[4];
             if (iz == 0) {
-                G[p] = T(0);
+                g[0] = g[1] = g[2] = g[3] = T(0);
+                st4(G + p, g);
                 return;
             }
             const size_t cb = (size_t)m * L * n2 + pi;
-            const double ut = tderiv(U + cb, iz, nz, n2, hdzi);
-            const double vt = tderiv(V + cb, iz, nz, n2, hdzi);
-            const double wt = tderiv(WW + cb, iz, nz, n2, hdzi);
-            double wkq = (double)Pq[p] * (double)ZX[p] + (double)Pr[p] * (double)ZY[p] - (double)WY[p] * vt;
-            wkq += ((double)UX[p] + (double)VY[p]) * wt - (double)WX[p] * ut;
-            G[p] = (T)wkq;
+            double ut[4], vt[4], wt[4];
+            tderiv4(U + cb, iz, nz, n2, hdzi, ut);
+            tderiv4(V + cb, iz, nz, n2, hdzi, vt);
+            tderiv4(WW + cb, iz, nz, n2, hdzi, wt);
+            T pq[4], pr[4], zx[4], zy[4], wx[4], wy[4], ux[4], vy[4];
+            ld4(Pq + p, pq);
+            ld4(Pr + p, pr);
+            ld4(ZX + p, zx);
+            ld4(ZY + p, zy);
+            ld4(WX + p, wx);
+            ld4(WY + p, wy);
+            ld4(UX + p, ux);
+            ld4(VY + p, vy);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                double wkq = (double)pq[e] * (double)zx[e] + (double)pr[e] * (double)zy[e] - (double)wy[e] * vt[e];
+                wkq += ((double)ux[e] + (double)vy[e]) * wt[e] - (double)wx[e] * ut[e];
+                g[e] = (T)wkq;
+            }
+            st4(G + p, g);
         });
         fft.ptospc(st, ML,
             [=] __device__(int q, int iy, int ix) -> T { return G[(size_t)q * n2 + iy + ng * ix]; },
@@ -1452,33 +1518,51 @@ struct Solver {
         fft.spctop(st, ML,
             [=] __device__(int q, int kx, int ky) -> T { return Sq2[(size_t)q * n2 + kx + ng * ky]; },
             [=] __device__(int q, int iy, int ix, T val) { Gq[(size_t)q * n2 + iy + ng * ix] = val; });
-        for_planes(st, ML, n2, [=] __device__(int q, int pi) {
+        for_planes4(st, ML, n2, [=] __device__(int q, int pi) {
             const int m = q / L, iz = q % L;
             const size_t p = (size_t)q * n2 + pi;
-            const T val = Gq[p];
-            const double ux = UX[p], uy = UY[p], vx = VX[p], vy = VY[p];
-            double s;
-            if (mixed) {
-                const double hz = HZ[p];
-                if (iz == 0) {
-                    s = hz + 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
-                } else {
-                    const double rip = RI[p];
-                    s = hz - COF * (rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
-                    s += 2.0 * (ux * vy - uy * vx);
-                }
-            } else {
-                const double hsv = (double)hsrc[(size_t)m * n2 + pi];
-                if (iz == 0) {
-                    s = hsv + COF * (double)ZE[p];
-                    s += 2.0 * (ux * vy - uy * vx + (double)Pq[p] * (ux + vy));
-                } else {
-                    const double rip = RI[p];
-                    s = hsv + COF * ((double)ZE[p] - rip * (double)Pp[p]) + 2.0 * (rip * (double)val);
-                    s += 2.0 * (ux * vy - uy * vx);
-                }
+            T gv[4], uxv[4], uyv[4], vxv[4], vyv[4], pqv[4], out[4];
+            ld4(Gq + p, gv);
+            ld4(UX + p, uxv);
+            ld4(UY + p, uyv);
+            ld4(VX + p, vxv);
+            ld4(VY + p, vyv);
+            T hv[4], riv[4], ppv[4], zev[4];
+            if (iz == 0) ld4(Pq + p, pqv);
+            if (mixed) ld4(HZ + p, hv);
+            else ld4(hsrc + (size_t)m * n2 + pi, hv);
+            if (iz != 0) {
+                ld4(RI + p, riv);
+                ld4(Pp + p, ppv);
             }
-            SP0[p] = (T)s;
+            if (!mixed) ld4(ZE + p, zev);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const double ux = uxv[e], uy = uyv[e], vx = vxv[e], vy = vyv[e];
+                double s;
+                if (mixed) {
+                    const double hz = hv[e];
+                    if (iz == 0) {
+                        s = hz + 2.0 * (ux * vy - uy * vx + (double)pqv[e] * (ux + vy));
+                    } else {
+                        const double rip = riv[e];
+                        s = hz - COF * (rip * (double)ppv[e]) + 2.0 * (rip * (double)gv[e]);
+                        s += 2.0 * (ux * vy - uy * vx);
+                    }
+                } else {
+                    const double hsv = (double)hv[e];
+                    if (iz == 0) {
+                        s = hsv + COF * (double)zev[e];
+                        s += 2.0 * (ux * vy - uy * vx + (double)pqv[e] * (ux + vy));
+                    } else {
+                        const double rip = riv[e];
+                        s = hsv + COF * ((double)zev[e] - rip * (double)ppv[e]) + 2.0 * (rip * (double)gv[e]);
+                        s += 2.0 * (ux * vy - uy * vx);
+                    }
+                }
+                out[e] = (T)s;
+            }
+            st4(SP0 + p, out);
         });
         int* ctl = ctrl.p;
         for_cols(st, M, [=] __device__(int m) {
