@@ -694,12 +694,20 @@ struct Solver {
             mean[2 * m] = uio;
             mean[2 * m + 1] = vio;
         });
-        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+        for_planes4(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L;
             const double uio = mean[2 * m], vio = mean[2 * m + 1];
             const size_t p = (size_t)q * n2 + i;
-            U[p] = (T)((double)U[p] + uio);
-            V[p] = (T)((double)V[p] + vio);
+            T uv[4], vv[4];
+            ld4(U + p, uv);
+            ld4(V + p, vv);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                uv[e] = (T)((double)uv[e] + uio);
+                vv[e] = (T)((double)vv[e] + vio);
+            }
+            st4(U + p, uv);
+            st4(V + p, vv);
         });
     }
 
@@ -1459,21 +1467,26 @@ struct Solver {
                 out[(size_t)q * n2 + iy + ng * ix] = val;
             });
         // P8: cpt1 = 0.5 d(cpt2)/dtheta + div(sig); sig *= 2 (coeffs.rs:44-100)
-        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+        //     (four elements per thread; the theta derivative is tderiv's one-sided /
+        //     centred form with qdzi)
+        for_planes4(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L, iz = q % L;
-            const T* c2 = C2 + (size_t)m * L * n2 + i;
             const size_t p = (size_t)q * n2 + i;
-            double val;
-            if (iz == 0)
-                val = qdzi * (4.0 * (double)c2[n2] - 3.0 * (double)c2[0] - (double)c2[2 * (size_t)n2]);
-            else if (iz < nz)
-                val = qdzi * ((double)c2[(size_t)(iz + 1) * n2] - (double)c2[(size_t)(iz - 1) * n2]) + (double)D[p];
-            else
-                val = qdzi * (3.0 * (double)c2[(size_t)nz * n2] + (double)c2[(size_t)(nz - 2) * n2] -
-                              4.0 * (double)c2[(size_t)(nz - 1) * n2]) + (double)D[p];
-            C1[p] = (T)val;
-            SIGX[p] = SIGX[p] * T(2);
-            SIGY[p] = SIGY[p] * T(2);
+            double t[4];
+            tderiv4(C2 + (size_t)m * L * n2 + i, iz, nz, n2, qdzi, t);
+            T dv[4], c1[4], sx[4], sy[4];
+            if (iz > 0) ld4(D + p, dv);
+            ld4(SIGX + p, sx);
+            ld4(SIGY + p, sy);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                c1[e] = (T)(iz == 0 ? t[e] : t[e] + (double)dv[e]);
+                sx[e] = sx[e] * T(2);
+                sy[e] = sy[e] * T(2);
+            }
+            st4(C1 + p, c1);
+            st4(SIGX + p, sx);
+            st4(SIGY + p, sy);
         });
         // P9/P10: the second dealiased product and sp0 (cpsource.rs:222-258), both
         // formed in streaming passes around plain transforms (staging in W(8), W(9))
@@ -1937,19 +1950,60 @@ struct Solver {
         // one streaming pass into staging planes (W(0..4), W(7): the pressure
         // sweep's work planes and F, all consumed by now), then transformed
         T *G0 = W(0), *G1 = W(1), *G2 = W(2), *G3 = W(3), *G4 = W(4), *G5 = W(7);
-        for_planes(st, ML, n2, [=] __device__(int q, int i) {
+        // (four elements per thread with 16-byte loads and stores; n2 % 4 == 0)
+        for_planes4(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L, iz = q % L;
             const size_t p = (size_t)q * n2 + i;
-            const T u = U[p], v = V[p], zx = ZX[p], zy = ZY[p], ff = FF[p], dd = DD[p];
-            const T qv = q_phys ? (T)((double)ZE[p] - COF * (double)R[p]) : Q[p];
-            G0[p] = qv * u;
-            G1[p] = qv * v;
-            const T bx = iz == 0 ? zx0[(size_t)m * n2 + i] : zx;
-            const T by = iz == 0 ? zy0[(size_t)m * n2 + i] : zy;
-            G2[p] = FX[p] * by - FY[p] * bx;
-            G3[p] = UX[p] * VY[p] - UY[p] * VX[p];
-            G4[p] = ff * zx - dd * u;
-            G5[p] = ff * zy - dd * v;
+            T u[4], v[4], zx[4], zy[4], ff[4], dd[4], qv[4], bx[4], by[4], fx[4], fy[4];
+            ld4(U + p, u);
+            ld4(V + p, v);
+            ld4(ZX + p, zx);
+            ld4(ZY + p, zy);
+            ld4(FF + p, ff);
+            ld4(DD + p, dd);
+            ld4(FX + p, fx);
+            ld4(FY + p, fy);
+            if (q_phys) {
+                T ze[4], rr[4];
+                ld4(ZE + p, ze);
+                ld4(R + p, rr);
+#pragma unroll
+                for (int e = 0; e < 4; e++) qv[e] = (T)((double)ze[e] - COF * (double)rr[e]);
+            } else {
+                ld4(Q + p, qv);
+            }
+            if (iz == 0) {
+                ld4(zx0 + (size_t)m * n2 + i, bx);
+                ld4(zy0 + (size_t)m * n2 + i, by);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    bx[e] = zx[e];
+                    by[e] = zy[e];
+                }
+            }
+            T g0[4], g1[4], g2[4], g4[4], g5[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                g0[e] = qv[e] * u[e];
+                g1[e] = qv[e] * v[e];
+                g2[e] = fx[e] * by[e] - fy[e] * bx[e];
+                g4[e] = ff[e] * zx[e] - dd[e] * u[e];
+                g5[e] = ff[e] * zy[e] - dd[e] * v[e];
+            }
+            st4(G0 + p, g0);
+            st4(G1 + p, g1);
+            st4(G2 + p, g2);
+            st4(G4 + p, g4);
+            st4(G5 + p, g5);
+            T ux[4], uy[4], vx[4], vy[4], g3[4];
+            ld4(UX + p, ux);
+            ld4(UY + p, uy);
+            ld4(VX + p, vx);
+            ld4(VY + p, vy);
+#pragma unroll
+            for (int e = 0; e < 4; e++) g3[e] = ux[e] * vy[e] - uy[e] * vx[e];
+            st4(G3 + p, g3);
         });
         fft.ptospc(st, 6 * ML,  // level-major
             [=] __device__(int o, int iy, int ix) -> T {
