@@ -246,6 +246,15 @@ __device__ __forceinline__ int mirror(int a, int ng) { return a == 0 ? 0 : ng - 
 __device__ __forceinline__ double dmul(int a, int ng) {
     return (a == 0 || 2 * a == ng) ? 0.0 : ((2 * a < ng) ? -(double)a : (double)(ng - a));
 }
+// dmul(a) * v in v's precision.  dmul is an integer of magnitude at most ng/2, so
+// the float64 product with a float value is exact and rounding it once to float
+// gives the float product itself: dmul_t(a, ng, v) == (T)(dmul(a, ng) * (double)v)
+// bit for bit, without the conversions and the float64 multiply.
+__device__ __forceinline__ int imul(int a, int ng) { return (a == 0 || 2 * a == ng) ? 0 : ((2 * a < ng) ? -a : ng - a); }
+template <typename T>
+__device__ __forceinline__ T dmul_t(int a, int ng, T v) {
+    return (T)imul(a, ng) * v;
+}
 // Parseval weight of one axis for the Hermitian packing: 1 at 0 and ng/2, else 2.
 __device__ __forceinline__ double pweight(int a, int ng) { return (a == 0 || 2 * a == ng) ? 1.0 : 2.0; }
 

@@ -757,8 +757,8 @@ struct Solver {
             [=] __device__(int o, int kx, int ky) -> T {
                 const int which = o / Mnz, q = o - which * Mnz, m = q / nz, iz = 1 + q % nz;
                 const T* s = S1 + (size_t)(m * L + iz) * n2;
-                if (which == 0) return (T)(dmul(kx, ng) * (double)s[mirror(kx, ng) + ng * ky]);
-                return (T)(dmul(ky, ng) * (double)s[kx + ng * mirror(ky, ng)]);
+                if (which == 0) return dmul_t(kx, ng, s[mirror(kx, ng) + ng * ky]);
+                return dmul_t(ky, ng, s[kx + ng * mirror(ky, ng)]);
             },
             [=] __device__(int o, int iy, int ix, T val) {
                 const int which = o / Mnz, q = o - which * Mnz, m = q / nz, iz = 1 + q % nz;
@@ -1009,8 +1009,8 @@ struct Solver {
             [=] __device__(int o, int kx, int ky) -> T {
                 const int which = o / ML, q = o - which * ML;
                 const T* s = (which < 2 ? Su : which < 4 ? Sv : Sw) + (size_t)q * n2;
-                if ((which & 1) == 0) return (T)(dmul(kx, ng) * (double)s[mirror(kx, ng) + ng * ky]);
-                return (T)(dmul(ky, ng) * (double)s[kx + ng * mirror(ky, ng)]);
+                if ((which & 1) == 0) return dmul_t(kx, ng, s[mirror(kx, ng) + ng * ky]);
+                return dmul_t(ky, ng, s[kx + ng * mirror(ky, ng)]);
             },
             [=] __device__(int o, int iy, int ix, T val) {
                 const int which = o / ML, q = o - which * ML;
@@ -1279,7 +1279,7 @@ struct Solver {
                 if (o < q_r) {  // z_x, z_y of one level adjacent
                     const int k = o - q_x, which = k & 1, kk = k >> 1, m = kk / nz, iz = 1 + kk % nz;
                     const T* sz = S1 + (size_t)(m * L + iz) * n2;
-                    return which == 0 ? (T)(dmul(kx, ng) * (double)sz[mx]) : (T)(dmul(ky, ng) * (double)sz[my]);
+                    return which == 0 ? dmul_t(kx, ng, sz[mx]) : dmul_t(ky, ng, sz[my]);
                 }
                 if (o < q_d) {
                     const int q = o - q_r;
@@ -1293,7 +1293,7 @@ struct Solver {
                 if (o < q_h) {  // u_x, u_y, v_x, v_y of one level adjacent
                     const int k = o - q_d, which = k & 3, q = k >> 2;
                     const T* sv = (which < 2 ? Su : Sv) + (size_t)q * n2;
-                    return (which & 1) == 0 ? (T)(dmul(kx, ng) * (double)sv[mx]) : (T)(dmul(ky, ng) * (double)sv[my]);
+                    return (which & 1) == 0 ? dmul_t(kx, ng, sv[mx]) : dmul_t(ky, ng, sv[my]);
                 }
                 if (!mixed) return hs[(size_t)(o - q_h) * n2 + i];
                 const int q = o - q_h, m = q / L;
@@ -1923,7 +1923,7 @@ struct Solver {
                 if (o >= nf2) {
                     const int which = (o - nf2) / M, m = (o - nf2) % M;
                     const T* s = zs0 + (size_t)m * n2;
-                    return which == 0 ? (T)(dmul(kx, ng) * (double)s[mx]) : (T)(dmul(ky, ng) * (double)s[my]);
+                    return which == 0 ? dmul_t(kx, ng, s[mx]) : dmul_t(ky, ng, s[my]);
                 }
                 const int q = o / nk, which = o - nk * q + q0;
                 if (which < 2) return (T)(which == 0 ? QS : DS)[(size_t)q * n2 + kx + ng * ky];
@@ -1931,8 +1931,8 @@ struct Solver {
                 const T* s = (w2 < 3 ? F : w2 < 5 ? Su : Sv) + (size_t)q * n2;
                 const int kind = w2 < 3 ? w2 : (w2 - 3) % 2 + 1;  // 0 value, 1 d/dx, 2 d/dy
                 if (kind == 0) return s[kx + ng * ky];
-                if (kind == 1) return (T)(dmul(kx, ng) * (double)s[mx]);
-                return (T)(dmul(ky, ng) * (double)s[my]);
+                if (kind == 1) return dmul_t(kx, ng, s[mx]);
+                return dmul_t(ky, ng, s[my]);
             },
             [=] __device__(int o, int iy, int ix, T val) {
                 const int i = iy + ng * ix;
