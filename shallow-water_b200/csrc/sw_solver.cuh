@@ -39,23 +39,25 @@ struct SweepMidLoad {
     static constexpr bool pair_io = true;
     const T* mid;
     int ng, nz;
-    __device__ __forceinline__ const T* row(int o, int kx, double& f) const {
+    // f is the integer d/dx factor (or 1), so f * v in T equals the rounded
+    // float64 product (as dmul_t)
+    __device__ __forceinline__ const T* row(int o, int kx, T& f) const {
         const int mm = o / (3 * nz), k = o - mm * 3 * nz, iz = k / 3, kind = k - 3 * iz;
         const int plane = mm * 2 * nz + 2 * iz + (kind == 2 ? 1 : 0);
-        f = kind == 1 ? dmul(kx, ng) : 1.0;
+        f = kind == 1 ? (T)imul(kx, ng) : T(1);
         return mid + ((size_t)plane * ng + (kind == 1 ? mirror(kx, ng) : kx)) * ng;
     }
     __device__ __forceinline__ T operator()(int o, int c, int p) const {
-        double f;
+        T f;
         const T* rw = row(o, p, f);
-        return (T)(f * (double)rw[c]);
+        return f * rw[c];
     }
     __device__ __forceinline__ T2 ld2(int o, int c, int p) const {
-        double f;
+        T f;
         const T* rw = row(o, p, f);
         T2 v = *reinterpret_cast<const T2*>(rw + c);
-        v.x = (T)(f * (double)v.x);
-        v.y = (T)(f * (double)v.y);
+        v.x = f * v.x;
+        v.y = f * v.y;
         return v;
     }
 };
