@@ -7,7 +7,7 @@ of q per grid point (delta = gamma = 0); one step = one predictor-corrector
 is no dataset.  All fields (>= 8.9 MB each, ~0.5 GB working set) exceed the
 126 MB L2, so no flush is needed between steps.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed|fp32]
     python bench.py --impl reference ...   (CPU FP64 oracle on the host cores)
 
 Multi-GPU (torchrun): one independent member per rank (replicas, weak scaling);
@@ -35,9 +35,11 @@ UNIT = "member-steps/s"
 # reverse passes of the transform micro-benchmark.  Reads are the plane data.  At
 # 102 planes the written planes mostly stay in the 126 MB L2 until after the
 # kernel; at 816 and 1632 planes most of them reach DRAM within it.
-FFT_PASS_DRAM_BYTES = {("mixed", 102): 26.86e6, ("fp64", 102): 60.4e6,
-                       ("mixed", 816): 377.7e6, ("mixed", 1632): 805.9e6,
-                       ("fp64", 816): 803.5e6, ("fp64", 1632): 1658.8e6}
+# Keys: (bytes per value of the pass, planes per launch).
+FFT_PASS_DRAM_BYTES = {(4, 102): 26.86e6, (8, 102): 60.4e6,
+                       (4, 816): 377.7e6, (4, 1632): 805.9e6,
+                       (8, 816): 803.5e6, (8, 1632): 1658.8e6}
+PRECISIONS = ("fp64", "mixed", "fp32")
 
 
 def load_package():
@@ -60,13 +62,17 @@ def initial_fields(ng, nz, seed, vstrip_fn):
     return q3, z3, z3.copy()
 
 
-def algorithmic_bytes_per_step(ng, nz, sweeps, w_fft):
+def algorithmic_bytes_per_step(ng, nz, sweeps, w_fft, corr_sweeps=0.0):
     """Algorithmic bytes of one advance step (member): one plane read + one plane
     write per 2-D transform of the reference's decomposition, plus the float64
-    Thomas traffic per pressure sweep.  sweeps = total psolve sweeps of the step."""
+    Thomas traffic per pressure sweep.  sweeps = psolve sweeps of the step in the
+    precision w_fft (bytes per value); corr_sweeps = float32 correction sweeps of
+    SW_MIXED (4-byte transforms, float32 Thomas input and correction)."""
     n2 = ng * ng
     ffts = 3 * (63 * nz + 47) + sweeps * (7 * nz + 1)
-    return ffts * 2 * n2 * w_fft + sweeps * (4 * nz + 2) * n2 * 8
+    fixed = ffts * 2 * n2 * w_fft + sweeps * (4 * nz + 2) * n2 * 8
+    corr = corr_sweeps * ((7 * nz + 1) * 2 * n2 * 4 + (nz + 1) * n2 * 4 + (2 * nz - 1) * n2 * 8 + 2 * nz * n2 * 4)
+    return fixed + corr
 
 
 class ClockSampler:
@@ -246,6 +252,10 @@ def fft_only(sw, sp, args, w_fft):
     return 0
 
 
+def prec_code(sw, name):
+    return {"fp64": sw.SW_FP64, "mixed": sw.SW_MIXED, "fp32": sw.SW_FP32}[name]
+
+
 def run_arm(sw, args, precision, rank, world, local, full=True):
     """Build an ensemble context, warm up, time `steps` advance steps on the device
     (CUDA events on the library's stream) and, when `full`, the end-to-end C-ABI
@@ -253,8 +263,8 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     member-0 prognostic fields after warmup + steps."""
     import torch
     L = sw._native.lib()
-    prec = sw.SW_FP64 if precision == "fp64" else sw.SW_MIXED
-    w_fft = 8 if prec == sw.SW_FP64 else 4
+    prec = prec_code(sw, precision)
+    w_fft = 4 if prec == sw.SW_FP32 else 8
     M = args.members
     sp = sw.Spectral(NG, NZ, precision=prec, nmembers=M, device=local)
     sw._native.check(L.sw_set_graphs(sp.ctx, 1 if args.graphs == "on" else 0))
@@ -286,27 +296,33 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     for _ in range(args.warmup):
         sw._native.check(L.sw_advance(sp.ctx, 1, 1))
     sw.nhswps.diag_history(sp)
-    sweeps_seen = []
     n0, n1 = ctypes.c_longlong(), ctypes.c_longlong()
+    c0, c1 = (ctypes.c_longlong * 2)(), (ctypes.c_longlong * 2)()
     barrier()
     torch.cuda.synchronize()
     sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n0)))
+    sw._native.check(L.sw_sweep_counts(sp.ctx, c0))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        # the K steps are queued as graph launches without a host round trip between
+        # them (sw_advance_async); one sw_sync after the end event collects the status
         e0.record(stream)
-        for _ in range(args.steps):
-            sw._native.check(L.sw_advance(sp.ctx, 1, 1))
-            sweeps_seen.append(sum(sw.nhswps.last_sweeps(sp)))
+        sw._native.check(L.sw_advance_async(sp.ctx, args.steps, 1))
         e1.record(stream)
+        sw._native.check(L.sw_sync(sp.ctx))
         torch.cuda.synchronize()
     barrier()
     sw._native.check(L.sw_kernel_launches(sp.ctx, ctypes.byref(n1)))
+    sw._native.check(L.sw_sweep_counts(sp.ctx, c1))
     ms = e0.elapsed_time(e1)
     t_local = ms / 1e3
+    ref_sweeps = (c1[0] - c0[0]) / args.steps
+    corr_sweeps = (c1[1] - c0[1]) / args.steps
     res = {
         "precision": precision, "w_fft": w_fft, "ms": ms, "t_local": t_local,
         "value": replica_throughput(args.steps * M, t_local, world, "cuda"),
-        "launches": int(n1.value - n0.value), "sweeps": float(np.mean(sweeps_seen)), "clocks": clk.summary(),
+        "launches": int(n1.value - n0.value), "sweeps": ref_sweeps + corr_sweeps,
+        "sweeps_float64": ref_sweeps, "sweeps_correction": corr_sweeps, "clocks": clk.summary(),
         "tune": tune,
         "snapshot": {k: st.get(k).ravel(order="F") for k in ("qs", "ds", "gs", "pn")},
     }
@@ -412,8 +428,8 @@ def drift(sw, args, rank, local):
     out = {"mode": "drift", "workload": "nhswps, one member, ng=%d nz=%d, vstrip + N(0,1e-3) q, delta=gamma=0"
                                          % (NG, NZ), "steps": args.drift, "ng": NG, "nz": NZ}
     finals = {}
-    for prec_name, prec in (("fp64", sw.SW_FP64), ("mixed", sw.SW_MIXED)):
-        sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+    for prec_name in PRECISIONS:
+        sp = sw.Spectral(NG, NZ, precision=prec_code(sw, prec_name), device=local)
         st = sw.nhswps.initial_state(sp, q3, d3, g3)
         sw.nhswps.psolve(st)  # z, w and p of the initial state, so that its energies are complete
         rec = []
@@ -443,9 +459,12 @@ def drift(sw, args, rank, local):
         }
         finals[prec_name] = {k: st.get(k).ravel(order="F") for k in ("qs", "ds", "gs")}
         sp.close()
-    out["mixed_vs_fp64_after"] = {k: float(np.linalg.norm(finals["mixed"][k] - finals["fp64"][k]) /
-                                          max(np.linalg.norm(finals["fp64"][k]), 1e-300)) for k in ("qs", "ds", "gs")}
-    out["etot_mixed_minus_fp64_rel"] = (out["mixed"]["etot_end"] - out["fp64"]["etot_end"]) / abs(out["fp64"]["etot_end"])
+    for name in ("mixed", "fp32"):
+        out[name + "_vs_fp64_after"] = {k: float(np.linalg.norm(finals[name][k] - finals["fp64"][k]) /
+                                                max(np.linalg.norm(finals["fp64"][k]), 1e-300))
+                                        for k in ("qs", "ds", "gs")}
+        out["etot_%s_minus_fp64_rel" % name] = ((out[name]["etot_end"] - out["fp64"]["etot_end"]) /
+                                               abs(out["fp64"]["etot_end"]))
     print(json.dumps(out), flush=True)
     return 0
 
@@ -463,7 +482,7 @@ def uneven(sw, args, rank, world, local):
     groups = {}
     for k, key in enumerate(draws):
         groups.setdefault(key, []).append(k)
-    prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
+    prec = prec_code(sw, args.precision)
     ctxs = []
     for (ng, nz), members in sorted(groups.items()):
         sp = sw.Spectral(ng, nz, precision=prec, nmembers=len(members), device=local)
@@ -554,7 +573,7 @@ def kernels(sw, args, rank, local):
     rng = np.random.default_rng(2)
     for n in (32, 96, 160, 256, 384, 512):
         m = 17 * n
-        for prec_name, prec, dt in (("fp64", sw.SW_FP64, torch.float64), ("fp32", sw.SW_MIXED, torch.float32)):
+        for prec_name, prec, dt in (("fp64", sw.SW_FP64, torch.float64), ("fp32", sw.SW_FP32, torch.float32)):
             x = torch.from_numpy(rng.standard_normal(m * n)).to(dt).cuda()
             xp = ctypes.c_void_p(x.data_ptr())
             nbytes = 2 * m * n * x.element_size()
@@ -589,8 +608,8 @@ def accuracy(sw, args, rank, local):
     qq2 = sw.vstrip.pv_strip(NG)
     q3, d3, g3 = initial_fields(NG, NZ, args.seed0, lambda ng: qq2)
     res, rates = {}, {}
-    for prec_name, prec in (("fp64", sw.SW_FP64), ("mixed", sw.SW_MIXED)):
-        sp = sw.Spectral(NG, NZ, precision=prec, device=local)
+    for prec_name in PRECISIONS:
+        sp = sw.Spectral(NG, NZ, precision=prec_code(sw, prec_name), device=local)
         st = sw.nhswps.initial_state(sp, q3, d3, g3)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -600,11 +619,12 @@ def accuracy(sw, args, rank, local):
         f["h"] = f["z"][-NG * NG:] / 0.4 - 1.0
         res[prec_name] = f
         sp.close()
-    err = {k: float(np.linalg.norm(res["mixed"][k] - res["fp64"][k]) / max(np.linalg.norm(res["fp64"][k]), 1e-300))
-           for k in res["fp64"]}
+    err = {name: {k: float(np.linalg.norm(res[name][k] - res["fp64"][k]) / max(np.linalg.norm(res["fp64"][k]), 1e-300))
+                  for k in res["fp64"]} for name in ("mixed", "fp32")}
     print(json.dumps({"mode": "accuracy", "ng": NG, "nz": NZ, "steps": args.steps,
                       "workload": "one member, vstrip + N(0,1e-3) q, delta=gamma=0",
-                      "mixed_rel_l2_vs_fp64": err, "steps_per_s_incl_first_graph_capture": rates}), flush=True)
+                      "mixed_rel_l2_vs_fp64": err["mixed"], "fp32_rel_l2_vs_fp64": err["fp32"],
+                      "steps_per_s_incl_first_graph_capture": rates}), flush=True)
     return 0
 
 
@@ -615,8 +635,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
-                    help="precision of the timed (headline) path")
+    ap.add_argument("--precision", default="mixed", choices=list(PRECISIONS),
+                    help="precision of the timed (headline) path: mixed = float64 with float32 pressure "
+                         "correction sweeps (the 1e-5 contract); fp32 = float32 transforms and work fields")
     ap.add_argument("--members", type=int, default=16, help="ensemble members per GPU (one batched context)")
     ap.add_argument("--compare", default="on", choices=["on", "off"],
                     help="also time the other precision on the same ensemble and report the ratio and the "
@@ -667,13 +688,13 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     sw = load_package()
     if args.fft_only:
-        prec = sw.SW_FP64 if args.precision == "fp64" else sw.SW_MIXED
+        prec = prec_code(sw, args.precision)
         # the intermediate holds 6 (nz+1) planes per member: enough members for --planes
         nmem = max(1, -(-args.planes // (6 * (NZ + 1))))
         sp = sw.Spectral(NG, NZ, precision=prec, nmembers=nmem, device=local)
         if args.fft_tile:
             sp.set_fft_tile(args.fft_tile)
-        return fft_only(sw, sp, args, 8 if prec == sw.SW_FP64 else 4)
+        return fft_only(sw, sp, args, 4 if prec == sw.SW_FP32 else 8)
     if args.kernels:
         return kernels(sw, args, rank, local)
     if args.accuracy:
@@ -684,9 +705,12 @@ def main():
         return uneven(sw, args, rank, world, local)
 
     main_arm = run_arm(sw, args, args.precision, rank, world, local, full=True)
-    other = None
+    arms = {args.precision: main_arm}
     if args.compare == "on":
-        other = run_arm(sw, args, "fp64" if args.precision == "mixed" else "mixed", rank, world, local, full=False)
+        # every rank runs the same arms in the same order (the barriers inside match)
+        for name in PRECISIONS:
+            if name not in arms:
+                arms[name] = run_arm(sw, args, name, rank, world, local, full=False)
 
     M = args.members
     w_fft = main_arm["w_fft"]
@@ -695,9 +719,9 @@ def main():
     achieved = fft["bytes"] / fft["per_launch_s"] / 1e9
     one = fft["one_member"]
     achieved_one = one["bytes"] / one["per_launch_s"] / 1e9
-    traffic = FFT_PASS_DRAM_BYTES.get((args.precision, fft["planes"])) if NG == 256 else None
-    traffic_one = FFT_PASS_DRAM_BYTES.get((args.precision, one["planes"])) if NG == 256 else None
-    step_bytes = algorithmic_bytes_per_step(NG, NZ, main_arm["sweeps"], w_fft)
+    traffic = FFT_PASS_DRAM_BYTES.get((w_fft, fft["planes"])) if NG == 256 else None
+    traffic_one = FFT_PASS_DRAM_BYTES.get((w_fft, one["planes"])) if NG == 256 else None
+    step_bytes = algorithmic_bytes_per_step(NG, NZ, main_arm["sweeps_float64"], w_fft, main_arm["sweeps_correction"])
     step_gbs = step_bytes * (args.steps * M / main_arm["t_local"]) / 1e9
 
     cpu = None
@@ -711,12 +735,23 @@ def main():
         line = {
             "metric": METRIC, "value": main_arm["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": main_arm["ms"] / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w_fft == 8 else "f32+f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp64": "f64", "mixed": "f64+f32", "fp32": "f32+f64"}[args.precision], "data": "synthetic",
             "config": {"workload": "nhswps advance, ng=%d nz=%d, batched ensemble, vstrip + N(0,1e-3) q "
                                    "(seed per member), delta=gamma=0" % (NG, NZ),
                        "ng": NG, "nz": NZ, "members_per_gpu": M, "precision": args.precision,
                        "parallelism": "replicas" if world > 1 else "single", "l2": "inputs larger than L2",
                        "psolve_sweeps_per_step": main_arm["sweeps"],
+                       "psolve_sweeps_per_step_float64": main_arm["sweeps_float64"],
+                       "psolve_sweeps_per_step_float32_correction": main_arm["sweeps_correction"],
+                       "timing": "K graph-launched steps queued without host round trips, CUDA events on the "
+                                 "library's stream",
+                       "precision_note": {"fp64": "float64 throughout",
+                                          "mixed": "float64 except the pressure iteration: after a float64 "
+                                                   "reference sweep, float32 correction sweeps on the distance "
+                                                   "from the reference point, stop rule 1e-7",
+                                          "fp32": "float32 transforms and work fields; not within 1e-5 on "
+                                                  "delta/gamma at ng=256"}[args.precision],
                        "fft_autotune": main_arm["tune"]},
             "e2e": main_arm["e2e"],
             "e2e_sequential": main_arm.get("e2e_sequential"),
@@ -731,18 +766,20 @@ def main():
             "cpu_baseline": cpu,
             "clocks": main_arm["clocks"],
         }
-        if other is not None:
-            mixed, fp64 = (main_arm, other) if args.precision == "mixed" else (other, main_arm)
-            line["compare"] = {
-                "fp64_value": fp64["value"], "mixed_value": mixed["value"],
-                "mixed_over_fp64": mixed["value"] / fp64["value"],
-                "fp64_sweeps_per_step": fp64["sweeps"], "mixed_sweeps_per_step": mixed["sweeps"],
-                "after_steps": args.warmup + args.steps,
-                "mixed_rel_l2_vs_fp64": {k: float(np.linalg.norm(mixed["snapshot"][k] - fp64["snapshot"][k]) /
-                                                  max(np.linalg.norm(fp64["snapshot"][k]), 1e-300))
-                                         for k in ("qs", "ds", "gs", "pn")},
-                "fp64_clocks": fp64["clocks"] if args.precision == "mixed" else main_arm["clocks"],
-            }
+        if len(arms) == len(PRECISIONS):
+            fp64 = arms["fp64"]
+            cmp = {"after_steps": args.warmup + args.steps, "fp64_value": fp64["value"],
+                   "fp64_sweeps_per_step": fp64["sweeps"], "fp64_clocks": fp64["clocks"]}
+            for name in ("mixed", "fp32"):
+                a = arms[name]
+                cmp[name + "_value"] = a["value"]
+                cmp[name + "_over_fp64"] = a["value"] / fp64["value"]
+                cmp[name + "_sweeps_per_step"] = {"float64": a["sweeps_float64"], "float32_correction":
+                                                  a["sweeps_correction"]}
+                cmp[name + "_rel_l2_vs_fp64"] = {k: float(np.linalg.norm(a["snapshot"][k] - fp64["snapshot"][k]) /
+                                                          max(np.linalg.norm(fp64["snapshot"][k]), 1e-300))
+                                                 for k in ("qs", "ds", "gs", "pn")}
+            line["compare"] = cmp
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

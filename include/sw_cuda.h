@@ -32,7 +32,16 @@ extern "C" {
 
 /* ---- precision of the hot path ---------------------------------------------- */
 #define SW_FP64 0  /* everything in float64 */
-#define SW_MIXED 1 /* float32 FFTs/products, float64 tridiagonal solve, residual, diagnostics, time update */
+/* float64 fields and transforms, except the pressure iteration: after a float64
+ * reference sweep, the sweeps of each solve are float32 correction sweeps on the
+ * distance from the reference point, with the float64 stop rule (1e-9), so the
+ * pressure converges as in SW_FP64 while most sweeps move half the bytes */
+#define SW_MIXED 1
+/* float32 transforms, products and physical work fields; float64 prognostic fields,
+ * tridiagonal solves, residual, diagnostics and time update; the pressure iteration
+ * stops at 1e-6 or on stagnation.  Fastest, but its gravity-wave fields (delta,
+ * gamma) carry ~1e-4 relative error after 10 steps at ng=256. */
+#define SW_FP32 2
 
 /* ---- fields of nhswps::State (src/nhswps/mod.rs:87-148) ------------------------ */
 enum sw_field {
@@ -55,7 +64,7 @@ int sw_initfft(int n, int factors[5], double* trig);
  * consistency with n when non-NULL; the GPU keeps its own twiddle tables. */
 int sw_forfft(int m, int n, double* x, const double* trig, const int factors[5]);
 int sw_revfft(int m, int n, double* x, const double* trig, const int factors[5]);
-/* Same on device memory: precision SW_FP64 (x is double*) or SW_MIXED (x is float*). */
+/* Same on device memory: precision SW_FP64 (x is double*), SW_MIXED or SW_FP32 (x is float*). */
 int sw_forfft_dev(int m, int n, void* x, int precision, void* stream);
 int sw_revfft_dev(int m, int n, void* x, int precision, void* stream);
 
@@ -125,6 +134,16 @@ int sw_advance(sw_ctx* ctx, int nsteps, int ggen);
  * conditional WHILE nodes (enable = 1, the default), or drive the iterations from
  * the host with one synchronisation per sweep (enable = 0).  Same results. */
 int sw_set_graphs(sw_ctx* ctx, int enable);
+/* Stop rule of the pressure iteration of an SW_MIXED context: the relative change
+ * below which psolve stops (default 1e-7; SW_FP64 keeps the reference's 1e-9,
+ * psolve.rs:17).  The correction sweeps converge below float32 rounding, so any
+ * value down to 1e-9 is reachable.  SW_ERR_STATE on other precisions.  No reference
+ * counterpart. */
+int sw_set_psolve_toler(sw_ctx* ctx, double toler);
+/* Pressure sweeps run on the context so far (each covers all members): out[0] float64
+ * sweeps (every sweep of SW_FP64 and SW_FP32, the reference sweeps of SW_MIXED),
+ * out[1] float32 correction sweeps of SW_MIXED.  No reference counterpart. */
+int sw_sweep_counts(sw_ctx* ctx, long long out[2]);
 /* Tuning of the batched 2-D transforms: planes per pair of tile-pass launches
  * (1 .. the context's capacity, 6*(nz+1)*nmembers; planes <= 0 only queries).
  * *in_use (may be NULL) gets the value now in use.  Results do not depend on it.  No reference counterpart:
@@ -176,7 +195,7 @@ int sw_sync(sw_ctx* ctx);
 
 /* ---- device-resident access for benchmarking and zero-copy callers ----------------- */
 /* Device pointer of a state field (all members, member-major) and its element size
- * in bytes (8 for the float64 fields; 4 for float32 fields of SW_MIXED). */
+ * in bytes (8 for the float64 fields; 4 for the float32 work fields of SW_FP32). */
 int sw_field_device_ptr(sw_ctx* ctx, int field, void** ptr, int* elem_bytes);
 /* Batched tridiagonal solves, float64: nsys independent systems of n <= 33
  * unknowns, a[i] x[i-1] + b[i] x[i] + c[i] x[i+1] = d[i] (a[0], c[n-1] unused),
@@ -192,7 +211,7 @@ int sw_tridiag_batched_host(int n, int nsys, const double* a, const double* b, c
 int sw_stream(sw_ctx* ctx, void** stream);
 /* Batched 2-D transforms on device memory with the context's plan: direction 0 =
  * ptospc (physical -> spectral), 1 = spctop; nplanes ng*ng planes of the context's
- * work precision (double for SW_FP64, float for SW_MIXED); in and out may alias.
+ * work precision (double for SW_FP64 and SW_MIXED, float for SW_FP32); in and out may alias.
  * Launches two tile passes per call (reference D2FFT::ptospc/spctop, src/sta2dfft.rs:91-123). */
 int sw_fft2d_dev(sw_ctx* ctx, int direction, int nplanes, const void* in, void* out);
 /* Allocation-free batched 2-D transforms (no counterpart in the reference).

@@ -67,6 +67,16 @@ def set_num_threads(n):
     lib().orc_set_num_threads(int(n))
 
 
+def set_fft_order(order):
+    """Radix schedule of the oracle's transforms for Spectral objects made after
+    this call: 0 (default) radix 4/2/3/5, 1 radix 5/3/2 (rounds differently)."""
+    lib().orc_set_fft_order(int(order))
+
+
+def get_fft_order():
+    return lib().orc_get_fft_order()
+
+
 # ---- stafft --------------------------------------------------------------
 def factorisen(n):
     f = (ctypes.c_int * 5)()

@@ -116,16 +116,31 @@ typedef struct {
     double *wr, *wi; /* cos/sin(2 pi t / n), t < n */
 } cplan;
 
+/* Radix schedule of the plans made from now on: 0 = radix 4, 2, 3, 5 in that
+ * order (the default); 1 = radix 2 in place of 4 and the order reversed (5, 3, 2).
+ * The second schedule rounds differently while computing the same transform: the
+ * spread between oracle runs under the two schedules is the float64 rounding floor
+ * against which GPU-vs-oracle differences are judged (test infrastructure only). */
+static int g_fft_order = 0;
+void orc_set_fft_order(int order) { g_fft_order = order; }
+int orc_get_fft_order(void) { return g_fft_order; }
+
 static int cplan_init(cplan* p, int n) {
     int rem = n;
     p->n = n;
     p->nrad = 0;
     p->wr = p->wi = NULL;
     if (n < 1) return ORC_ERR_ARG;
-    while (rem % 4 == 0) { p->rad[p->nrad++] = 4; rem /= 4; }
-    while (rem % 2 == 0) { p->rad[p->nrad++] = 2; rem /= 2; }
-    while (rem % 3 == 0) { p->rad[p->nrad++] = 3; rem /= 3; }
-    while (rem % 5 == 0) { p->rad[p->nrad++] = 5; rem /= 5; }
+    if (g_fft_order == 0) {
+        while (rem % 4 == 0) { p->rad[p->nrad++] = 4; rem /= 4; }
+        while (rem % 2 == 0) { p->rad[p->nrad++] = 2; rem /= 2; }
+        while (rem % 3 == 0) { p->rad[p->nrad++] = 3; rem /= 3; }
+        while (rem % 5 == 0) { p->rad[p->nrad++] = 5; rem /= 5; }
+    } else {
+        while (rem % 5 == 0) { p->rad[p->nrad++] = 5; rem /= 5; }
+        while (rem % 3 == 0) { p->rad[p->nrad++] = 3; rem /= 3; }
+        while (rem % 2 == 0) { p->rad[p->nrad++] = 2; rem /= 2; }
+    }
     if (rem != 1) return ORC_ERR_FACTORISE;
     p->wr = (double*)xmalloc(sizeof(double) * n);
     p->wi = (double*)xmalloc(sizeof(double) * n);

@@ -14,7 +14,7 @@ HEADER = os.path.join(HERE, "..", "include", "sw_cuda.h")
 
 SW_OK, SW_ERR_FACTORISE, SW_ERR_CUDA = 0, 1, 2
 SW_ERR_PSOLVE_DIVERGED, SW_ERR_PSOLVE_MAXITER, SW_ERR_ARG, SW_ERR_STATE = 3, 4, 6, 7
-SW_FP64, SW_MIXED = 0, 1
+SW_FP64, SW_MIXED, SW_FP32 = 0, 1, 2
 FIELDS = ["u", "v", "w", "z", "zx", "zy", "r", "ri", "aa", "zeta",
           "pn", "dpn", "ps", "qs", "ds", "gs"]
 FIELD_INDEX = {k: i for i, k in enumerate(FIELDS)}
@@ -65,6 +65,8 @@ _SIGS = {
     "sw_advance": (_i, [_vp, _i, _i]),
     "sw_set_graphs": (_i, [_vp, _i]),
     "sw_set_fft_chunk": (_i, [_vp, _i, _ip]),
+    "sw_set_psolve_toler": (_i, [_vp, ctypes.c_double]),
+    "sw_sweep_counts": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "sw_advance_async": (_i, [_vp, _i, _i]),
     "sw_savegrid": (_i, [_vp, _i, _dp, _dp, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "sw_state_set_all_async": (_i, [_vp, _i, _dp, _sz]),

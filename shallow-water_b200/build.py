@@ -15,6 +15,8 @@ NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo", "--extended-lambda",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC", "-shared",
+    # device-side optimisation of the compilation unit runs on all host cores
+    "-split-compile=0",
 ]
 
 

@@ -263,7 +263,7 @@ int sw_ctx_create(int ng, int nz, int nmembers, int precision, int device, sw_ct
     return guarded([&] {
         require(out != nullptr, SW_ERR_ARG, "null output pointer");
         *out = nullptr;
-        require(precision == SW_FP64 || precision == SW_MIXED, SW_ERR_ARG, "unknown precision");
+        require(precision == SW_FP64 || precision == SW_MIXED || precision == SW_FP32, SW_ERR_ARG, "unknown precision");
         int ndev = 0;
         SW_CUDA(cudaGetDeviceCount(&ndev));
         require(device >= 0 && device < ndev, SW_ERR_ARG, "no such CUDA device");
@@ -271,8 +271,12 @@ int sw_ctx_create(int ng, int nz, int nmembers, int precision, int device, sw_ct
         auto* c = new sw_ctx();
         c->ng = ng; c->nz = nz; c->M = nmembers; c->precision = precision; c->device = device;
         try {
-            if (precision == SW_FP64) c->s64.reset(new Solver<double>(ng, nz, nmembers));
-            else c->s32.reset(new Solver<float>(ng, nz, nmembers));
+            if (precision == SW_FP32) {
+                c->s32.reset(new Solver<float>(ng, nz, nmembers));
+            } else {
+                c->s64.reset(new Solver<double>(ng, nz, nmembers));
+                if (precision == SW_MIXED) c->s64->enable_refine32();
+            }
         } catch (...) {
             delete c;
             throw;
@@ -712,6 +716,21 @@ int sw_stream(sw_ctx* ctx, void** stream) {
 int sw_set_graphs(sw_ctx* ctx, int enable) {
     return with_solver(ctx, [&](auto& s) {
         s.use_graphs = enable != 0;
+        return SW_OK;
+    });
+}
+int sw_sweep_counts(sw_ctx* ctx, long long out[2]) {
+    return with_solver(ctx, [&](auto& s) {
+        require(out != nullptr, SW_ERR_ARG, "null output");
+        if (s.pending) s.advance_finish();
+        out[0] = s.sweeps_run[0];
+        out[1] = s.sweeps_run[1];
+        return SW_OK;
+    });
+}
+int sw_set_psolve_toler(sw_ctx* ctx, double toler) {
+    return with_solver(ctx, [&](auto& s) {
+        s.set_refine_toler(toler);
         return SW_OK;
     });
 }

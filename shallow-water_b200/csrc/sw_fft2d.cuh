@@ -184,6 +184,7 @@ struct Fft2d {
     FftPlan plan{};
     DevBuf<T2> tw;
     DevBuf<T> mid;
+    T* midp = nullptr;  // the intermediate: mid, or storage lent by the owner
     int cap = 0;    // planes the intermediate holds
     int chunk = 0;  // planes per pair of pass launches (<= cap)
     int tc = 2;
@@ -197,14 +198,20 @@ struct Fft2d {
         return c < 1 ? 1 : (c > cap ? cap : c);
     }
 
-    void init(int ng_, int cap_planes) {
+    // lent: storage of at least cap_planes ng*ng planes of T that the caller owns
+    // and never uses while a transform of this object is queued (nullptr: allocate)
+    void init(int ng_, int cap_planes, T* lent = nullptr) {
         ng = ng_;
         require(build_plan(ng, plan) == SW_OK, SW_ERR_FACTORISE, "grid size must factor into 2, 3, 5");
         auto h = host_twiddles<T>(ng);
         tw.alloc(ng);
         SW_CUDA(cudaMemcpy(tw.p, h.data(), sizeof(T2) * ng, cudaMemcpyHostToDevice));
         cap = cap_planes;
-        mid.alloc((size_t)cap * ng * ng);
+        if (lent) midp = lent;
+        else {
+            mid.alloc((size_t)cap * ng * ng);
+            midp = mid.p;
+        }
         chunk = default_chunk(ng, cap);
         // n = 256: the register-staged pass (16- or 32-column tiles, one buffer)
         tc = ng == FFT_R_N ? 2 * fft_r_np<T>() : pick_tile<T>(ng);
@@ -226,16 +233,16 @@ struct Fft2d {
     void spctop(cudaStream_t s, int nout, LD ld, ST st) const {
         for (int o0 = 0; o0 < nout; o0 += chunk) {
             const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
-            launch_pass<T, true, true, false>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidPC<T>{mid.p, ng});
-            launch_pass<T, true, true, true>(s, plan, tw.p, tc, sc, cnt, ng, MidCP<T>{mid.p, ng}, StOff<ST>{st, o0});
+            launch_pass<T, true, true, false>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidPC<T>{midp, ng});
+            launch_pass<T, true, true, true>(s, plan, tw.p, tc, sc, cnt, ng, MidCP<T>{midp, ng}, StOff<ST>{st, o0});
         }
     }
     template <class LD, class ST>
     void ptospc(cudaStream_t s, int nout, LD ld, ST st) const {
         for (int o0 = 0; o0 < nout; o0 += chunk) {
             const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
-            launch_pass<T, false, true, true>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidCP<T>{mid.p, ng});
-            launch_pass<T, false, false, true>(s, plan, tw.p, tc, sc, cnt, ng, MidPC<T>{mid.p, ng}, StOff<ST>{st, o0});
+            launch_pass<T, false, true, true>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidCP<T>{midp, ng});
+            launch_pass<T, false, false, true>(s, plan, tw.p, tc, sc, cnt, ng, MidPC<T>{midp, ng}, StOff<ST>{st, o0});
         }
     }
 };

@@ -104,8 +104,9 @@ __global__ void k_spec_bins(int nbins, const int* __restrict__ off, const int* _
 // in registers (same arithmetic as the streamed loop in psolve_finish).
 template <typename T, int NZS>
 __global__ void __launch_bounds__(128)
-k_dpdtheta(int n2, int ncols, const double* __restrict__ PS, const T* __restrict__ SP, const double* __restrict__ htd1,
-           const double* __restrict__ etd1, double hdzi, double dzi, double dz6, double* __restrict__ GG) {
+k_dpdtheta(int n2, int ncols, const double* __restrict__ PS, const T* __restrict__ SP, const float* __restrict__ SPC,
+           const double* __restrict__ htd1, const double* __restrict__ etd1, double hdzi, double dzi, double dz6,
+           double* __restrict__ GG) {
     const int c = blockIdx.x * 128 + threadIdx.x;
     if (c >= ncols) return;
     const int m = c / n2, i = c - m * n2;
@@ -113,7 +114,7 @@ k_dpdtheta(int n2, int ncols, const double* __restrict__ PS, const T* __restrict
     double p[NZS + 1], g[NZS + 1];
 #pragma unroll
     for (int iz = 0; iz <= NZS; iz++) p[iz] = PS[cb + (size_t)iz * n2];
-    const double spn = (double)SP[cb + (size_t)NZS * n2];
+    const double spn = (double)SP[cb + (size_t)NZS * n2] + (SPC ? (double)SPC[cb + (size_t)NZS * n2] : 0.0);
     g[0] = 0.0;
     g[1] = (p[2] - p[0]) * hdzi * htd1[0];
 #pragma unroll
@@ -200,22 +201,45 @@ k_update(int n2, int ncols, double dt4, double dt4i, const double* __restrict__ 
 
 constexpr int THOMAS_THREADS = 128;
 
+// Block sum of NV per-thread values into part[(m * gridDim.x + blockIdx.x) * NV + v].
+template <int NV>
+__device__ __forceinline__ void block_partials(const double (&v)[NV], int m, double* part) {
+    __shared__ double sh[NV][THOMAS_THREADS];
+#pragma unroll
+    for (int k = 0; k < NV; k++) sh[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int w = THOMAS_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+#pragma unroll
+            for (int k = 0; k < NV; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) part[((size_t)m * gridDim.x + blockIdx.x) * NV + k] = sh[k][0];
+    }
+}
+
 // Compact fourth-order RHS and Thomas solve of one sweep (psolve.rs:285-327) for
 // one (kx, ky) column per thread; member = blockIdx.y.  Writes ps and the new
 // previous-iterate psa, and reduces the Parseval-weighted sums of
-// (ps - psa_old)^2 and psa_old^2 per CTA into part[(m*gridDim.x + blk)*2 + {0,1}].
+// (ps - psa_old)^2 and psa_old^2 per CTA into part[(m*gridDim.x + blk)*NV + {0,1}].
 // NZS > 0: compile-time nz; the column is kept in registers between the forward
 // elimination and the back substitution (ps is written once).
-template <typename T, int NZS>
+// NV = 3 (the reference sweeps of the mixed path) also writes the change of the
+// sweep, D1 = ps_new - ps_old for levels 0..nz-1 in float32, and reduces the
+// weighted sum of ps_new^2 into part[... + 2].
+template <typename T, int NZS, int NV>
 __global__ void __launch_bounds__(THOMAS_THREADS)
 k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __restrict__ SP,
          const double* __restrict__ htdv, const double* __restrict__ etdv, const double* __restrict__ ap,
-         double* __restrict__ PS, double* __restrict__ XF, double* __restrict__ part) {
+         double* __restrict__ PS, double* __restrict__ XF, float* __restrict__ D1, double* __restrict__ part) {
     const int m = blockIdx.y;
     const int i = blockIdx.x * THOMAS_THREADS + threadIdx.x;
     const int nz = NZS ? NZS : nz_rt;
     const int L = nz + 1;
-    double sn = 0.0, sd = 0.0;
+    double sn = 0.0, sd = 0.0, sx = 0.0;
     if (NZS && i < n2 && ctl[3 * m]) {
         const size_t cb = (size_t)m * L * n2 + i;
         const double api = ap[i];
@@ -243,6 +267,10 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
             sn += (x[iz] - old[iz]) * (x[iz] - old[iz]);
             sd += old[iz] * old[iz];
             PS[cb + (size_t)iz * n2] = x[iz];
+            if (NV == 3) {
+                sx += x[iz] * x[iz];
+                D1[cb + (size_t)iz * n2] = (float)(x[iz] - old[iz]);
+            }
         }
         sn += old[NZS] * old[NZS];
         sd += old[NZS] * old[NZS];
@@ -251,6 +279,7 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
         const double wgt = pweight(kx, ng) * pweight(ky, ng);
         sn *= wgt;
         sd *= wgt;
+        sx *= wgt;
     } else if (!NZS && i < n2 && ctl[3 * m]) {
         const size_t cb = (size_t)m * L * n2 + i;
         const double api = ap[i];
@@ -280,6 +309,10 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
             sn += (xn - old) * (xn - old);
             sd += old * old;
             PS[p] = xn;
+            if (NV == 3) {
+                sx += xn * xn;
+                D1[p] = (float)(xn - old);
+            }
         }
 #pragma unroll 4
         for (int iz = nz - 2; iz >= 0; iz--) {
@@ -289,44 +322,140 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
             sn += (xi - old) * (xi - old);
             sd += old * old;
             PS[p] = xi;
+            if (NV == 3) {
+                sx += xi * xi;
+                D1[p] = (float)(xi - old);
+            }
             xn = xi;
         }
         const int kx = i % ng, ky = i / ng;
         const double wgt = pweight(kx, ng) * pweight(ky, ng);
         sn *= wgt;
         sd *= wgt;
+        sx *= wgt;
     }
-    __shared__ double sh[2][THOMAS_THREADS];
-    sh[0][threadIdx.x] = sn;
-    sh[1][threadIdx.x] = sd;
-    __syncthreads();
-    for (int w = THOMAS_THREADS / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+    if constexpr (NV == 3) {
+        const double v[3] = {sn, sd, sx};
+        block_partials<3>(v, m, part);
+    } else {
+        const double v[2] = {sn, sd};
+        block_partials<2>(v, m, part);
+    }
+}
+
+// Thomas solve of a float32 correction sweep of the mixed path: the compact RHS of
+// the correction source SP32 (float32, levels 0..nz) and the solve in float64
+// arithmetic give the correction c = T^-1 SP32 of the pressure against the last
+// reference sweep's result (which ps holds).  The previous correction C is replaced;
+// the weighted sum of (c_new - c_old)^2 goes to part[... * 3 + 0] (the numerator of
+// errp; the control kernel divides by the reference sweep's sum of ps^2).
+template <int NZS>
+__global__ void __launch_bounds__(THOMAS_THREADS)
+k_thomas_c(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const float* __restrict__ SP32,
+           const double* __restrict__ htdv, const double* __restrict__ etdv, const double* __restrict__ ap,
+           float* __restrict__ Cr, double* __restrict__ XF, double* __restrict__ part) {
+    const int m = blockIdx.y;
+    const int i = blockIdx.x * THOMAS_THREADS + threadIdx.x;
+    const int nz = NZS ? NZS : nz_rt;
+    const int L = nz + 1;
+    double sn = 0.0;
+    if (NZS && i < n2 && ctl[3 * m]) {
+        const size_t cb = (size_t)m * L * n2 + i;
+        const double api = ap[i];
+        double sp[NZS ? NZS + 1 : 1], x[NZS ? NZS : 1], ed[NZS ? NZS : 1], old[NZS ? NZS : 1];
+#pragma unroll
+        for (int iz = 0; iz <= NZS; iz++) sp[iz] = (double)SP32[cb + (size_t)iz * n2];
+#pragma unroll
+        for (int iz = 0; iz < NZS; iz++) x[iz] = htdv[i + (size_t)n2 * iz];
+#pragma unroll
+        for (int iz = 0; iz + 1 < NZS; iz++) ed[iz] = etdv[i + (size_t)n2 * iz];
+#pragma unroll
+        for (int iz = 0; iz < NZS; iz++) old[iz] = (double)Cr[cb + (size_t)iz * n2];
+        x[0] = ((1.0 / 3.0) * sp[0] + (1.0 / 6.0) * sp[1]) * x[0];
+#pragma unroll
+        for (int iz = 1; iz < NZS; iz++) {
+            const double g = (1.0 / 12.0) * (sp[iz - 1] + sp[iz + 1]) + (5.0 / 6.0) * sp[iz];
+            x[iz] = (g - api * x[iz - 1]) * x[iz];
         }
-        __syncthreads();
+#pragma unroll
+        for (int iz = NZS - 2; iz >= 0; iz--) x[iz] += ed[iz] * x[iz + 1];
+#pragma unroll
+        for (int iz = 0; iz < NZS; iz++) {
+            sn += (x[iz] - old[iz]) * (x[iz] - old[iz]);
+            Cr[cb + (size_t)iz * n2] = (float)x[iz];
+        }
+        const int kx = i % ng, ky = i / ng;
+        sn *= pweight(kx, ng) * pweight(ky, ng);
+    } else if (!NZS && i < n2 && ctl[3 * m]) {
+        const size_t cb = (size_t)m * L * n2 + i;
+        const double api = ap[i];
+        double spm = (double)SP32[cb], spc = (double)SP32[cb + n2];
+        double x = ((1.0 / 3.0) * spm + (1.0 / 6.0) * spc) * htdv[i];
+        XF[cb] = x;
+#pragma unroll 4
+        for (int iz = 1; iz < nz; iz++) {
+            const double spp = (double)SP32[cb + (size_t)(iz + 1) * n2];
+            const double g = (1.0 / 12.0) * (spm + spp) + (5.0 / 6.0) * spc;
+            x = (g - api * x) * htdv[i + (size_t)n2 * iz];
+            XF[cb + (size_t)iz * n2] = x;
+            spm = spc;
+            spc = spp;
+        }
+        double xn = x;
+        {
+            const size_t p = cb + (size_t)(nz - 1) * n2;
+            const double old = (double)Cr[p];
+            sn += (xn - old) * (xn - old);
+            Cr[p] = (float)xn;
+        }
+#pragma unroll 4
+        for (int iz = nz - 2; iz >= 0; iz--) {
+            const size_t p = cb + (size_t)iz * n2;
+            const double xi = XF[p] + etdv[i + (size_t)n2 * iz] * xn;
+            const double old = (double)Cr[p];
+            sn += (xi - old) * (xi - old);
+            Cr[p] = (float)xi;
+            xn = xi;
+        }
+        const int kx = i % ng, ky = i / ng;
+        sn *= pweight(kx, ng) * pweight(ky, ng);
     }
-    if (threadIdx.x == 0) {
-        part[((size_t)m * gridDim.x + blockIdx.x) * 2] = sh[0][0];
-        part[((size_t)m * gridDim.x + blockIdx.x) * 2 + 1] = sh[1][0];
-    }
+    const double v[3] = {sn, 0.0, 0.0};
+    block_partials<3>(v, m, part);
 }
 
 constexpr int CTRL_THREADS = 256;
 constexpr int CTRL_MAX_MEMBERS = 256;
 
-// Stop rule of one member (psolve.rs:89, 339-366).
-__device__ __forceinline__ void ctrl_member(int m, double a, double b, int* ctl, double* errp, double toler,
-                                                 int mixed, int nitmax, int* any) {
+// Stop rule of one member (psolve.rs:89, 339-366).  One deliberate deviation: a
+// relative change that is not finite (a NaN or an infinity anywhere in the member's
+// pressure) ends the member's iteration with SW_ERR_PSOLVE_DIVERGED at any sweep.
+// The reference's loop condition `while errp > toler` (psolve.rs:88) is false for a
+// NaN, so there a non-finite state leaves the loop as if it had converged.
+//
+// Correction sweeps (kind != null, the mixed path): kind_now says whether the sweep
+// just run was a float64 reference sweep (0) or a float32 correction sweep (1).  A
+// reference sweep records its relative change in eref[m].  A member that goes on
+// iterating asks for a new reference sweep (*want64) once its correction sweeps have
+// stopped shrinking the change by 30% per sweep, or have shrunk it by 1e-6 against
+// that record: the float32 rounding of a correction is relative to the distance from
+// the reference point, so a nearer reference point lowers that floor.
+//
+// For a correction sweep the relative change is (weighted) |c_new - c_old| / |p1|,
+// with |p1|^2 (the sum c of the reference sweep) kept in pnorm[m]: p1 + c_old is the
+// previous iterate and |c_old| is small next to |p1|.
+__device__ __forceinline__ void ctrl_member(int m, double a, double b, double c, int* ctl, double* errp,
+                                                 double toler, int mixed, int nitmax, int* any, const int* kind,
+                                                 int kind_now, double* eref, double* pnorm, int* want64) {
     {
         if (!ctl[3 * m]) return;
-        const double e = sqrt(a / (b + 1.0E-20));
+        if (kind && kind_now == 0) pnorm[m] = c;
+        const double e = (kind && kind_now == 1) ? sqrt(a / (pnorm[m] + 1.0E-20)) : sqrt(a / (b + 1.0E-20));
         const double eprev = ctl[3 * m + 1] > 0 ? errp[m] : 1.0;
         const bool stagnated = mixed && e < 1.0E-4 && e > 0.7 * eprev;
         errp[m] = e;
         const int it = ctl[3 * m + 1];
-        if (it > 0 && e > 1.0) {
+        if (!isfinite(e) || (it > 0 && e > 1.0)) {
             ctl[3 * m + 2] = SW_ERR_PSOLVE_DIVERGED;
             ctl[3 * m] = 0;
             ctl[3 * m + 1] = it + 1;
@@ -338,6 +467,10 @@ __device__ __forceinline__ void ctrl_member(int m, double a, double b, int* ctl,
             if (it + 1 >= nitmax && !(mixed && (!(e > toler) || stagnated))) ctl[3 * m + 2] = SW_ERR_PSOLVE_MAXITER;
         } else {
             atomicOr(any, 1);
+            if (kind) {
+                if (kind_now == 0) eref[m] = e;
+                else if (e < 1.0E-6 * eref[m] || e > 0.7 * eprev) atomicOr(want64, 1);
+            }
         }
     }
 }
@@ -350,43 +483,65 @@ __device__ __forceinline__ void ctrl_member(int m, double a, double b, int* ctl,
 // float32 transforms put a floor of ~1e-6 under that change, so the mixed path
 // stops at 1e-6, or earlier once the change has stagnated (< 1e-4 and no longer
 // shrinking by 30% per sweep).
-__global__ void k_psolve_ctrl(int M, int nblk, const double* __restrict__ part, int* ctl, double* errp, double toler,
-                              int mixed, int nitmax, int use_cond, cudaGraphConditionalHandle cond,
-                              long long* nexec) {
-    __shared__ int any;
-    __shared__ double sums[2 * CTRL_MAX_MEMBERS];
-    if (threadIdx.x == 0) any = 0;
+// With kind set (the mixed path's correction sweeps), the kind of the next sweep is
+// written to kind[0] and, inside a graph, to the conditions c64 / c32 of the two
+// conditional sweep bodies.
+// Partials: NV = 2 values per CTA (sn, sd), or 3 with the correction sweeps (sn,
+// sd, sum of ps^2 of a reference sweep; sn alone for a correction sweep).
+static __global__ void k_psolve_ctrl(int M, int nblk, int nv, const double* __restrict__ part, int* ctl, double* errp,
+                                     double toler, int mixed, int nitmax, int use_cond, cudaGraphConditionalHandle cond,
+                                     long long* nexec, int* kind, double* eref, double* pnorm,
+                                     cudaGraphConditionalHandle c64, cudaGraphConditionalHandle c32) {
+    __shared__ int any, want64;
+    __shared__ double sums[3 * CTRL_MAX_MEMBERS];
+    const int kind_now = kind ? kind[0] : 0;
+    if (threadIdx.x == 0) {
+        any = 0;
+        want64 = 0;
+    }
     // one warp per member: lane-strided partial sums, then a fixed shuffle tree
     // (deterministic order)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = CTRL_THREADS / 32;
     for (int m0 = 0; m0 < M; m0 += CTRL_MAX_MEMBERS) {
         const int mcount = (M - m0 < CTRL_MAX_MEMBERS) ? M - m0 : CTRL_MAX_MEMBERS;
         for (int mm = warp; mm < mcount; mm += nwarps) {
-            const double* pm = part + (size_t)(m0 + mm) * nblk * 2;
-            double a = 0.0, b = 0.0;
+            const double* pm = part + (size_t)(m0 + mm) * nblk * nv;
+            double a = 0.0, b = 0.0, c = 0.0;
 #pragma unroll 8
             for (int k = lane; k < nblk; k += 32) {
-                a += pm[2 * k];
-                b += pm[2 * k + 1];
+                a += pm[nv * k];
+                b += pm[nv * k + 1];
+                if (nv == 3) c += pm[nv * k + 2];
             }
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) {
                 a += __shfl_down_sync(0xffffffffu, a, off);
                 b += __shfl_down_sync(0xffffffffu, b, off);
+                c += __shfl_down_sync(0xffffffffu, c, off);
             }
             if (lane == 0) {
-                sums[2 * mm] = a;
-                sums[2 * mm + 1] = b;
+                sums[3 * mm] = a;
+                sums[3 * mm + 1] = b;
+                sums[3 * mm + 2] = c;
             }
         }
         __syncthreads();
-        for (int mm = threadIdx.x; mm < mcount; mm += CTRL_THREADS) ctrl_member(m0 + mm, sums[2 * mm], sums[2 * mm + 1],
-                                                                                 ctl, errp, toler, mixed, nitmax, &any);
+        for (int mm = threadIdx.x; mm < mcount; mm += CTRL_THREADS)
+            ctrl_member(m0 + mm, sums[3 * mm], sums[3 * mm + 1], sums[3 * mm + 2], ctl, errp, toler, mixed, nitmax,
+                        &any, kind, kind_now, eref, pnorm, &want64);
         __syncthreads();
     }
-    if (threadIdx.x == 0 && use_cond) {
-        *nexec = *nexec + 1;
-        cudaGraphSetConditional(cond, any ? 1u : 0u);
+    if (threadIdx.x == 0) {
+        const int next = (kind_now == 1 && want64) ? 0 : 1;
+        if (kind) kind[0] = next;
+        if (use_cond) {
+            nexec[kind_now] += 1;  // sweep bodies executed, per kind
+            cudaGraphSetConditional(cond, any ? 1u : 0u);
+            if (kind) {
+                cudaGraphSetConditional(c64, (any && next == 0) ? 1u : 0u);
+                cudaGraphSetConditional(c32, (any && next == 1) ? 1u : 0u);
+            }
+        }
     }
 }
 
@@ -425,8 +580,25 @@ struct Solver {
     DevBuf<int> sweeps_dev;  // per member: sweep counts of the 3 psolve calls of the last step
     DevBuf<int> err_dev;     // sticky status of captured steps
     DevBuf<int> hist_dev;    // diagnostics rows recorded since the last read
-    DevBuf<long long> sweep_exec;  // sweep bodies executed by graph launches (launch accounting)
-    long long k_fixed[2] = {0, 0}, k_sweep = 0;  // kernels per step outside the sweeps, per sweep
+    DevBuf<long long> sweep_exec;  // sweep bodies executed by graph launches, per kind (launch accounting)
+    long long k_fixed[2] = {0, 0};  // kernels per step outside the sweep loops
+    long long k_sweep = 0;          // kernels captured in one sweep loop body (both kinds)
+    long long k_sweep_kind[2] = {0, 0};  // kernels a body runs when it is a reference / correction sweep
+    // Mixed path: float32 correction sweeps on the float64 solver (T = double)
+    bool refine32 = false;
+    Fft2d<float> f32;          // float32 transforms (intermediate lent by fft)
+    // 11 float32 fields: 0..3 sweep planes (p, p_x, p_y, S1), 4 the correction source
+    // SP32, 5..8 coefficient copies (sigx, sigy, cpt2, cpt1), 9 the last reference
+    // sweep's change D1, 10 the correction C (the iterate is ps + C)
+    DevBuf<float> r32;
+    DevBuf<double> eref;       // per member: relative change of the last reference sweep
+    DevBuf<double> pnorm;      // per member: weighted |ps|^2 after the last reference sweep
+    double refine_toler = 1.0E-7;  // stop rule of the correction sweeps
+    DevBuf<int> sweep_kind;    // kind of the next sweep: 0 reference (float64), 1 correction (float32)
+    cudaStream_t st_if = nullptr;
+    int host_kind = 0;         // host-driven loops: kind of the next sweep
+    long long sweeps_run[2] = {0, 0};  // sweep launches so far: reference (float64) and correction (float32)
+    float* R32(int i) { return r32.p + (size_t)i * nf; }
     int last_sweeps[3] = {0, 0, 0};
 
     static constexpr int NWT = 24;
@@ -490,11 +662,12 @@ struct Solver {
         ctrl.alloc((size_t)3 * M + 1);
         SW_CUDA(cudaMallocHost(&h_pinned, sizeof(double) * (16 * (size_t)M + 64)));
         SW_CUDA(cudaStreamCreateWithFlags(&st_body, cudaStreamNonBlocking));
+        SW_CUDA(cudaStreamCreateWithFlags(&st_if, cudaStreamNonBlocking));
         sweeps_dev.alloc((size_t)3 * M);
         err_dev.alloc(1);
         hist_dev.alloc(1);
-        sweep_exec.alloc(1);
-        SW_CUDA(cudaMemset(sweep_exec.p, 0, sizeof(long long)));
+        sweep_exec.alloc(2);
+        SW_CUDA(cudaMemset(sweep_exec.p, 0, 2 * sizeof(long long)));
         SW_CUDA(cudaMemset(sweeps_dev.p, 0, sizeof(int) * 3 * M));
         SW_CUDA(cudaMemset(err_dev.p, 0, sizeof(int)));
         SW_CUDA(cudaMemset(hist_dev.p, 0, sizeof(int)));
@@ -503,9 +676,52 @@ struct Solver {
         if (st) cudaStreamSynchronize(st);
         for (auto& e : step_exec)
             if (e) cudaGraphExecDestroy(e);
+        if (st_if) cudaStreamDestroy(st_if);
         if (st_body) cudaStreamDestroy(st_body);
         if (h_pinned) cudaFreeHost(h_pinned);
         if (st) cudaStreamDestroy(st);
+    }
+
+    // The mixed path on the float64 solver: pressure sweeps after the first of each
+    // solve are float32 correction sweeps (sweep_correction), with float64 reference
+    // sweeps wherever the control kernel asks for one.  Everything else stays float64.
+    void enable_refine32() {
+        if constexpr (sizeof(T) == 8) {
+            if (refine32) return;
+            f32.init(ng, 2 * fft.cap, reinterpret_cast<float*>(fft.midp));
+            f32.set_chunk(f32.cap);
+            r32.alloc((size_t)11 * nf);
+            SW_CUDA(cudaMemset(r32.p, 0, sizeof(float) * 11 * nf));
+            eref.alloc(M);
+            SW_CUDA(cudaMemset(eref.p, 0, sizeof(double) * M));
+            pnorm.alloc(M);
+            SW_CUDA(cudaMemset(pnorm.p, 0, sizeof(double) * M));
+            sweep_kind.alloc(1);
+            SW_CUDA(cudaMemset(sweep_kind.p, 0, sizeof(int)));
+            SW_CUDA(cudaStreamSynchronize(st));
+            for (auto& e : step_exec)
+                if (e) {
+                    SW_CUDA(cudaGraphExecDestroy(e));
+                    e = nullptr;
+                }
+            refine32 = true;
+        } else {
+            require(false, SW_ERR_ARG, "correction sweeps need the float64 solver");
+        }
+    }
+
+    // Stop rule of the correction sweeps (the mixed path); the captured step graphs
+    // hold the old value, so they are dropped.
+    void set_refine_toler(double toler) {
+        require(refine32, SW_ERR_STATE, "the pressure tolerance is set on SW_MIXED contexts only");
+        require(toler > 0.0 && toler < 1.0, SW_ERR_ARG, "tolerance must be in (0, 1)");
+        SW_CUDA(cudaStreamSynchronize(st));
+        for (auto& e : step_exec)
+            if (e) {
+                SW_CUDA(cudaGraphExecDestroy(e));
+                e = nullptr;
+            }
+        refine_toler = toler;
     }
 
     // Planes per 2-D transform launch pair; the captured step graphs hold the old
@@ -1114,6 +1330,7 @@ struct Solver {
         (void)nitmax;
         if (fused_prepare) {
             psolve_prepare_fused();
+            prepare_refine();
             return;
         }
         const int ng = this->ng, n2 = this->n2, ML = this->ML;
@@ -1146,6 +1363,39 @@ struct Solver {
             ctl[3 * m + 1] = 0;
             ctl[3 * m + 2] = SW_OK;
         });
+        prepare_refine();
+    }
+
+    // Mixed path: float32 copies of the sweep coefficients for the correction sweeps,
+    // and the first sweep of the solve is a reference sweep.
+    void prepare_refine() {
+        host_kind = 0;
+        if constexpr (sizeof(T) == 8) {
+            if (!refine32) return;
+            const int n2 = this->n2, ML = this->ML;
+            const double *SX = sigx, *SY = sigy, *CC2 = cpt2, *CC1 = cpt1;
+            float *X = R32(5), *Y = R32(6), *Z2 = R32(7), *Z1 = R32(8), *Cr = R32(10);
+            int* kd = sweep_kind.p;
+            for_planes4(st, ML, n2, [=] __device__(int q, int i) {
+                const size_t p = (size_t)q * n2 + i;
+                if (q == 0 && i == 0) kd[0] = 0;
+                double v[4];
+                float f[4] = {0.f, 0.f, 0.f, 0.f};
+                st4(Cr + p, f);
+                ld4(SX + p, v);
+                for (int e = 0; e < 4; e++) f[e] = (float)v[e];
+                st4(X + p, f);
+                ld4(SY + p, v);
+                for (int e = 0; e < 4; e++) f[e] = (float)v[e];
+                st4(Y + p, f);
+                ld4(CC2 + p, v);
+                for (int e = 0; e < 4; e++) f[e] = (float)v[e];
+                st4(Z2 + p, f);
+                ld4(CC1 + p, v);
+                for (int e = 0; e < 4; e++) f[e] = (float)v[e];
+                st4(Z1 + p, f);
+            });
+        }
     }
 
     // psolve's set-up with vertical, coeffs and cpsource fused into eight large
@@ -1589,64 +1839,90 @@ struct Solver {
 
     // One pressure sweep (psolve.rs:89-358) and its convergence control.  With
     // cond set, the sweep is the body of a graph WHILE node and the last kernel
-    // sets the node's condition from the members still iterating.
-    void psolve_sweep(int nitmax, bool use_cond, cudaGraphConditionalHandle cond) {
-        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
-        const bool mixed = sizeof(T) == 4;
-        const double toler = mixed ? 1.0E-6 : 1.0E-9;
-        const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz2 = dz / 2.0, dz6 = dz / 6.0;
+    // sets the node's condition from the members still iterating.  With the
+    // correction sweeps on (the mixed path), the body is two conditional nodes, a
+    // float64 reference sweep and a float32 correction sweep, of which the control
+    // kernel enables one for the next iteration (c64, c32); host-driven loops pass
+    // the kind that the control kernel chose (host_kind).
+    void psolve_sweep(int nitmax, bool use_cond, cudaGraphConditionalHandle cond, cudaGraphConditionalHandle c64 = 0,
+                      cudaGraphConditionalHandle c32 = 0) {
+        if (!refine32) {
+            sweep_reference();
+        } else if (use_cond) {
+            const long long c0 = launch_counter().load();
+            capture_if(c64, [&] { sweep_reference(); });
+            const long long c1 = launch_counter().load();
+            capture_if(c32, [&] { sweep_correction(); });
+            k_sweep_kind[0] = c1 - c0 + 1;  // + the control kernel
+            k_sweep_kind[1] = launch_counter().load() - c1 + 1;
+        } else if (host_kind == 0) {
+            sweep_reference();
+        } else {
+            sweep_correction();
+        }
+        sweep_ctrl(nitmax, use_cond, cond, c64, c32);
+    }
+
+    // Captures body() into an IF node of the graph being captured on st, enabled
+    // by handle h (made in the enclosing step graph, set by the control kernel).
+    template <class F>
+    void capture_if(cudaGraphConditionalHandle h, F&& body) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        SW_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+        require(cs == cudaStreamCaptureStatusActive, SW_ERR_STATE, "capture_if outside a capture");
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cn;
+        SW_CUDA(cudaGraphAddNode(&cn, g, deps, nd, &cp));
+        cudaGraph_t body_graph = cp.conditional.phGraph_out[0];
+        SW_CUDA(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
+        cudaStream_t outer = st;
+        st = st_if;
+        SW_CUDA(cudaStreamBeginCaptureToGraph(st, body_graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        try {
+            body();
+        } catch (...) {
+            cudaGraph_t dummy;
+            cudaStreamEndCapture(st, &dummy);
+            st = outer;
+            throw;
+        }
+        cudaGraph_t done;
+        SW_CUDA(cudaStreamEndCapture(st, &done));
+        st = outer;
+    }
+
+    // The total source S = S0 + S1(p) of one sweep in physical space (psolve.rs:
+    // 96-240), TS-precision planes: A, B, C hold p, p_x, p_y of levels 0..nz-1; the
+    // theta derivatives are formed here.  SP0 == nullptr leaves S0 out (S1 alone: the
+    // correction sweeps).  S reads eight fields per element; as a streaming pass at
+    // full occupancy it runs near the memory bandwidth, while inside the transform's
+    // loader (sixteen pairs per thread, four CTAs per SM) the loads wait on latency.
+    // Four elements per thread with 16-byte loads and stores (n2 % 4 == 0: ng is even).
+    template <typename TS>
+    void sweep_source(const TS* A, const TS* B, const TS* C, const TS* SP0, const TS* SIGX, const TS* SIGY,
+                      const TS* C2, const TS* C1, TS* SRC) {
+        const int n2 = this->n2, L = this->L, nz = this->nz, ML = this->ML;
+        const double dz = HBAR / (double)nz, dz2 = dz / 2.0;
         const double dzisq = (1.0 / dz) * (1.0 / dz);
         const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
-        const double *filt = op.filt, *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap, *htd1 = op.htd1, *etd1 = op.etd1;
-        T *R = r, *RI = ri, *PN = pn, *DPN = dpn;
-        double* PS = ps;
-        T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
-        T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
-        double* XF = WD(1);
-        int* ctl = ctrl.p;
-        double* errp = errp_d.p;
-        (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;
-        (void)SIGX; (void)SIGY; (void)C1; (void)C2; (void)SP0; (void)A; (void)B; (void)C; (void)D; (void)ctl; (void)errp;
-        (void)htdv; (void)etdv; (void)ap; (void)dz2; (void)dzisq; (void)hdzi; (void)mixed;
-        // (a) p, dp/dx, dp/dy to physical space for levels 0..nz-1 (p(nz) = 0).  The
-        //     theta derivatives of the reference (psolve.rs:96-240) are linear in p,
-        //     so they are formed from these in physical space in (b): 3 nz transforms
-        //     per member instead of the 4 nz - 1 of the derived quantities.
-        //     d/dx acts on kx, which the first (reverse, along ky) pass leaves alone, so
-        //     p_x takes p's intermediate with the derivative applied in the second
-        //     pass: 2 nz first passes and 3 nz second passes per member.
-        const int n2z = 2 * nz;
-        const int mchunk = std::max(1, std::min(M, fft.chunk / n2z));
-        for (int m0 = 0; m0 < M; m0 += mchunk) {
-            const int mc = std::min(mchunk, M - m0);
-            launch_pass<T, true, true, false>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, n2z * mc, ng,
-                [=] __device__(int o, int kx, int ky) -> T {  // p, p_y of one level adjacent
-                    const int mm = o / n2z, k = o - mm * n2z, iz = k >> 1, kind = k & 1;
-                    const double* pc = PS + (size_t)((m0 + mm) * L + iz) * n2;
-                    if (kind == 0) return (T)pc[kx + ng * ky];
-                    return (T)(dmul(ky, ng) * pc[kx + ng * mirror(ky, ng)]);
-                },
-                MidPC<T>{fft.mid.p, ng});
-            launch_pass<T, true, true, true>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, 3 * nz * mc, ng,
-                SweepMidLoad<T>{fft.mid.p, ng, nz}, SweepPhysStore<T>{A, B, C, ng, nz, L, m0});
-        }
-        // (b) total source S = S0 + S1(p) in physical space, then to spectral space.
-        //     S reads eight fields per element; as a streaming pass at full occupancy
-        //     it runs near the memory bandwidth, while inside the transform's loader
-        //     (sixteen pairs per thread, four CTAs per SM) the loads wait on latency.
-        // Four elements per thread with 16-byte loads and stores (n2 % 4 == 0: ng is even).
-        T* SRC = D;
         for_planes4(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L, iz = q % L;
             const size_t p = (size_t)q * n2 + i;
             const size_t cb = (size_t)m * L * n2 + i;
-            T out[4];
+            TS out[4];
             if (iz > 0 && iz < nz) {
-                auto lv = [&](const T* f, int l, T(&v)[4]) {
-                    if (l >= nz) v[0] = v[1] = v[2] = v[3] = T(0);
+                auto lv = [&](const TS* f, int l, TS(&v)[4]) {
+                    if (l >= nz) v[0] = v[1] = v[2] = v[3] = TS(0);
                     else ld4(f + cb + (size_t)l * n2, v);
                 };
-                T xp[4], xm[4], yp[4], ym[4], pp[4], pc[4], pm[4], sp0[4], sx[4], sy[4], c2[4], c1[4];
+                TS xp[4], xm[4], yp[4], ym[4], pp[4], pc[4], pm[4], sp0[4], sx[4], sy[4], c2[4], c1[4];
                 lv(B, iz + 1, xp);
                 lv(B, iz - 1, xm);
                 lv(C, iz + 1, yp);
@@ -1654,7 +1930,8 @@ struct Solver {
                 lv(A, iz + 1, pp);
                 lv(A, iz, pc);
                 lv(A, iz - 1, pm);
-                ld4(SP0 + p, sp0);
+                if (SP0) ld4(SP0 + p, sp0);
+                else sp0[0] = sp0[1] = sp0[2] = sp0[3] = TS(0);
                 ld4(SIGX + p, sx);
                 ld4(SIGY + p, sy);
                 ld4(C2 + p, c2);
@@ -1667,7 +1944,7 @@ struct Solver {
                     const double d2 = ((double)pp[e] - 2.0 * (double)pc[e] + (double)pm[e]) * dzisq;
                     double s = (double)sp0[e] + (double)sx[e] * dxt + (double)sy[e] * dyt;
                     s += (double)c2[e] * d2 + (double)c1[e] * dpdt;
-                    out[e] = (T)s;
+                    out[e] = (TS)s;
                 }
             } else {
 #pragma unroll
@@ -1676,10 +1953,11 @@ struct Solver {
                     auto P = [&](int l) { return l >= nz ? 0.0 : (double)A[ce + (size_t)l * n2]; };
                     auto X = [&](int l) { return l >= nz ? 0.0 : (double)B[ce + (size_t)l * n2]; };
                     auto Y = [&](int l) { return l >= nz ? 0.0 : (double)C[ce + (size_t)l * n2]; };
+                    const double s0 = SP0 ? (double)SP0[pe] : 0.0;
                     double s;
                     if (iz == 0) {
                         const double d2 = (2.0 * P(0) - 5.0 * P(1) + 4.0 * P(2) - P(3)) * dzisq;
-                        s = (double)SP0[pe] + (double)C2[pe] * d2;
+                        s = s0 + (double)C2[pe] * d2;
                     } else {
                         // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238)
                         auto ext = [&](auto F) {
@@ -1692,67 +1970,198 @@ struct Solver {
                         const double d1 = (P(nz) - 2.0 * P(nz - 1) + P(nz - 2)) * dzisq;
                         const double d2 = (P(nz - 1) - 2.0 * P(nz - 2) + P(nz - 3)) * dzisq;
                         const double d2pdt2 = 2.0 * d1 - d2;
-                        s = (double)SP0[pe] + (double)SIGX[pe] * dxt + (double)SIGY[pe] * dyt;
+                        s = s0 + (double)SIGX[pe] * dxt + (double)SIGY[pe] * dyt;
                         s += (double)C2[pe] * d2pdt2 + (double)C1[pe] * dpdt;
                     }
-                    out[e] = (T)s;
+                    out[e] = (TS)s;
                 }
             }
             st4(SRC + p, out);
         });
-        fft.ptospc(st, ML,
-            [=] __device__(int q, int iy, int ix) -> T { return SRC[(size_t)q * n2 + iy + ng * ix]; },
-            [=] __device__(int q, int kx, int ky, T val) { SP[(size_t)q * n2 + kx + ng * ky] = val; });
-        // (c) compact RHS and Thomas solve per (kx, ky) column, with the errp sums
-        //     reduced per CTA; (d) one control kernel finishes the sums per member and
-        //     applies the stop rule (psolve.rs:89, 285-358)
+    }
+
+    // Compact RHS and Thomas solve per (kx, ky) column (psolve.rs:285-329), with the
+    // errp sums reduced per CTA.  With the correction sweeps on, the reference
+    // sweep's solve also records its change D1 and |ps|^2 (NV = 3).
+    void sweep_thomas(const T* SP) {
+        const int ng = this->ng, n2 = this->n2, nz = this->nz, M = this->M;
+        const double *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap;
+        double* PS = ps;
+        double* XF = WD(1);
+        const int* ctl = ctrl.p;
         const int nblk = (n2 + THOMAS_THREADS - 1) / THOMAS_THREADS;
         double* part = red_partial.p;
-        {
-            const dim3 g(nblk, M);
-            switch (nz) {
-                case 4: k_thomas<T, 4><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
-                case 8: k_thomas<T, 8><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
-                case 16: k_thomas<T, 16><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
-                case 32: k_thomas<T, 32><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
-                default: k_thomas<T, 0><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, part); break;
-            }
+        const dim3 g(nblk, M);
+        float* D1 = refine32 ? R32(9) : nullptr;
+#define SW_THOMAS_CASE(NZV)                                                                                      \
+    if (refine32)                                                                                                \
+        k_thomas<T, NZV, 3><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, D1, part); \
+    else                                                                                                         \
+        k_thomas<T, NZV, 2><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, D1, part);
+        switch (nz) {
+            case 4: SW_THOMAS_CASE(4) break;
+            case 8: SW_THOMAS_CASE(8) break;
+            case 16: SW_THOMAS_CASE(16) break;
+            case 32: SW_THOMAS_CASE(32) break;
+            default: SW_THOMAS_CASE(0) break;
         }
+#undef SW_THOMAS_CASE
         SW_CHECK_LAUNCH();
         count_launch();
-        k_psolve_ctrl<<<1, CTRL_THREADS, 0, st>>>(M, nblk, part, ctl, errp, toler, mixed ? 1 : 0, nitmax, use_cond ? 1 : 0,
-                                         cond, sweep_exec.p);
+    }
+
+    // The control kernel of one sweep: finishes the errp sums per member and applies
+    // the stop rule (psolve.rs:89, 339-358).  Stop rule: float64, the reference's 1e-9
+    // on the relative change; the correction sweeps, refine_toler; float32, 1e-6 or
+    // stagnation (see ctrl_member).
+    void sweep_ctrl(int nitmax, bool use_cond, cudaGraphConditionalHandle cond, cudaGraphConditionalHandle c64,
+                    cudaGraphConditionalHandle c32) {
+        const bool mixed = sizeof(T) == 4;
+        const double toler = mixed ? 1.0E-6 : (refine32 ? refine_toler : 1.0E-9);
+        const int nblk = (n2 + THOMAS_THREADS - 1) / THOMAS_THREADS;
+        k_psolve_ctrl<<<1, CTRL_THREADS, 0, st>>>(M, nblk, refine32 ? 3 : 2, red_partial.p, ctrl.p, errp_d.p, toler,
+                                                  mixed ? 1 : 0, nitmax, use_cond ? 1 : 0, cond, sweep_exec.p,
+                                                  refine32 ? sweep_kind.p : nullptr, eref.p, pnorm.p, c64, c32);
         SW_CHECK_LAUNCH();
         count_launch();
+    }
+
+    // Correction sweeps: the iterate is ps + C.  Folds C into ps (C = 0) and, with
+    // clear_sp32, clears the correction source, so that a reference sweep starts
+    // from the current iterate and a finished solve leaves it in ps.
+    void fold_correction(bool clear_sp32) {
+        const int n2 = this->n2, ML = this->ML;
+        double* PS = ps;
+        float *Cr = R32(10), *SPC = R32(4);
+        for_planes4(st, ML, n2, [=] __device__(int q, int i) {
+            const size_t p = (size_t)q * n2 + i;
+            double v[4];
+            float c[4];
+            ld4(PS + p, v);
+            ld4(Cr + p, c);
+            for (int e = 0; e < 4; e++) v[e] += (double)c[e];
+            st4(PS + p, v);
+            const float z[4] = {0.f, 0.f, 0.f, 0.f};
+            st4(Cr + p, z);
+            if (clear_sp32) st4(SPC + p, z);
+        });
+    }
+
+    // A sweep in the precision of T.  (a) p, dp/dx, dp/dy to physical space for
+    // levels 0..nz-1 (p(nz) = 0).  The theta derivatives of the reference
+    // (psolve.rs:96-240) are linear in p, so they are formed from these in physical
+    // space in (b): 3 nz transforms per member instead of the 4 nz - 1 of the derived
+    // quantities.  d/dx acts on kx, which the first (reverse, along ky) pass leaves
+    // alone, so p_x takes p's intermediate with the derivative applied in the second
+    // pass: 2 nz first passes and 3 nz second passes per member.  (b) the total source
+    // S = S0 + S1(p) in physical space, then to spectral space; (c) the Thomas solve.
+    // With the correction sweeps on, this is the reference sweep: it starts from the
+    // current iterate ps + C, and its solve p1 stays in ps while correction sweeps
+    // run; SP keeps the spectrum of S at the reference point p_ref.
+    void sweep_reference() {
+        const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+        double* PS = ps;
+        T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
+        if (refine32) fold_correction(true);
+        const int n2z = 2 * nz;
+        const int mchunk = std::max(1, std::min(M, fft.chunk / n2z));
+        for (int m0 = 0; m0 < M; m0 += mchunk) {
+            const int mc = std::min(mchunk, M - m0);
+            launch_pass<T, true, true, false>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, n2z * mc, ng,
+                [=] __device__(int o, int kx, int ky) -> T {  // p, p_y of one level adjacent
+                    const int mm = o / n2z, k = o - mm * n2z, iz = k >> 1, kind = k & 1;
+                    const double* pc = PS + (size_t)((m0 + mm) * L + iz) * n2;
+                    if (kind == 0) return (T)pc[kx + ng * ky];
+                    return (T)(dmul(ky, ng) * pc[kx + ng * mirror(ky, ng)]);
+                },
+                MidPC<T>{fft.midp, ng});
+            launch_pass<T, true, true, true>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, 3 * nz * mc, ng,
+                SweepMidLoad<T>{fft.midp, ng, nz}, SweepPhysStore<T>{A, B, C, ng, nz, L, m0});
+        }
+        sweep_source<T>(A, B, C, sp0.p, sigx.p, sigy.p, cpt2.p, cpt1.p, D);
+        fft.ptospc(st, ML,
+            [=] __device__(int q, int iy, int ix) -> T { return D[(size_t)q * n2 + iy + ng * ix]; },
+            [=] __device__(int q, int kx, int ky, T val) { SP[(size_t)q * n2 + kx + ng * ky] = val; });
+        sweep_thomas(SP);
+    }
+
+    // A float32 correction sweep of the mixed path (float64 solver only).  Apart
+    // from S0 the sweep is linear in p, and so is the Thomas solve T^-1: with p_ref
+    // the last reference sweep's input and p1 = T^-1 S(p_ref) its result (in ps), the
+    // next iterate is p1 + c with c = T^-1 S1(d), d = p - p_ref = D1 + C the distance
+    // of the current iterate p = p1 + C from p_ref.  The sweep transforms d (and its x,
+    // y derivatives) in float32, forms S1(d) with float32 copies of the coefficients
+    // and solves for the new C.  Its rounding is relative to |d|, which is small next
+    // to |p|, so the iteration converges well below float32 rounding of p while moving
+    // about half the bytes of a float64 sweep.
+    void sweep_correction() {
+        if constexpr (sizeof(T) == 8) {
+            const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
+            const float *D1 = R32(9), *Cr = R32(10);
+            float *A = R32(0), *B = R32(1), *C = R32(2), *D = R32(3), *SPC = R32(4);
+            const int n2z = 2 * nz;
+            const int mchunk = std::max(1, std::min(M, f32.chunk / n2z));
+            for (int m0 = 0; m0 < M; m0 += mchunk) {
+                const int mc = std::min(mchunk, M - m0);
+                launch_pass<float, true, true, false>(st, f32.plan, f32.tw.p, f32.tc, f32.sc, n2z * mc, ng,
+                    [=] __device__(int o, int kx, int ky) -> float {  // d, d_y of one level adjacent
+                        const int mm = o / n2z, k = o - mm * n2z, iz = k >> 1, kind = k & 1;
+                        const size_t b = (size_t)((m0 + mm) * L + iz) * n2;
+                        if (kind == 0) {
+                            const size_t j = b + kx + ng * ky;
+                            return D1[j] + Cr[j];
+                        }
+                        const size_t j = b + kx + ng * mirror(ky, ng);
+                        return dmul_t(ky, ng, D1[j] + Cr[j]);
+                    },
+                    MidPC<float>{f32.midp, ng});
+                launch_pass<float, true, true, true>(st, f32.plan, f32.tw.p, f32.tc, f32.sc, 3 * nz * mc, ng,
+                    SweepMidLoad<float>{f32.midp, ng, nz}, SweepPhysStore<float>{A, B, C, ng, nz, L, m0});
+            }
+            sweep_source<float>(A, B, C, nullptr, R32(5), R32(6), R32(7), R32(8), D);
+            f32.ptospc(st, ML,
+                [=] __device__(int q, int iy, int ix) -> float { return D[(size_t)q * n2 + iy + ng * ix]; },
+                [=] __device__(int q, int kx, int ky, float val) { SPC[(size_t)q * n2 + kx + ng * ky] = val; });
+            const double *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap;
+            const int* ctl = ctrl.p;
+            const int nblk = (n2 + THOMAS_THREADS - 1) / THOMAS_THREADS;
+            const dim3 g(nblk, M);
+            float* Cw = R32(10);
+            double *XF = WD(1), *part = red_partial.p;
+            switch (nz) {
+                case 4: k_thomas_c<4><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
+                case 8: k_thomas_c<8><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
+                case 16: k_thomas_c<16><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
+                case 32: k_thomas_c<32><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
+                default: k_thomas_c<0><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
+            }
+            SW_CHECK_LAUNCH();
+            count_launch();
+        }
     }
 
     // pn and dp/dtheta after convergence (psolve.rs:367-410).
     void psolve_finish() {
         const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
-        const bool mixed = sizeof(T) == 4;
-        const double toler = mixed ? 1.0E-6 : 1.0E-9;
-        const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz2 = dz / 2.0, dz6 = dz / 6.0;
-        const double dzisq = (1.0 / dz) * (1.0 / dz);
+        const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz6 = dz / 6.0;
         const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
-        const double *filt = op.filt, *htdv = op.htdv, *etdv = op.etdv, *ap = op.ap, *htd1 = op.htd1, *etd1 = op.etd1;
-        T *R = r, *RI = ri, *PN = pn, *DPN = dpn;
+        const double *htd1 = op.htd1, *etd1 = op.etd1;
+        T *PN = pn, *DPN = dpn;
         double* PS = ps;
-        T *SIGX = sigx, *SIGY = sigy, *C1 = cpt1, *C2 = cpt2, *SP0 = sp0;
-        T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
-        int* ctl = ctrl.p;
-        double* errp = errp_d.p;
-        (void)R; (void)RI; (void)filt; (void)toler; (void)dzi; (void)dz6; (void)htd1; (void)etd1; (void)PN; (void)DPN;
-        (void)SIGX; (void)SIGY; (void)C1; (void)C2; (void)SP0; (void)A; (void)B; (void)C; (void)D; (void)ctl; (void)errp;
-        (void)htdv; (void)etdv; (void)ap; (void)dz2; (void)dzisq; (void)hdzi; (void)mixed;
+        const T* SP = W(4);
+        // correction sweeps: the iterate ps + C into ps; the last sweep's source at
+        // level nz is SP + SP32 (SP32 is zero when that sweep was a reference sweep)
+        if (refine32) fold_correction(false);
+        const float* SPC = refine32 ? R32(4) : nullptr;
         // dp/dtheta by 4th-order compact differences (psolve.rs:371-410), levels 1..nz
         double* GG = WD(1);
         const int ncols = M * n2, nbk = (ncols + 127) / 128;
         bool done = true;
         switch (nz) {
-            case 4: k_dpdtheta<T, 4><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
-            case 8: k_dpdtheta<T, 8><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
-            case 16: k_dpdtheta<T, 16><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
-            case 32: k_dpdtheta<T, 32><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            case 4: k_dpdtheta<T, 4><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, SPC, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            case 8: k_dpdtheta<T, 8><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, SPC, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            case 16: k_dpdtheta<T, 16><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, SPC, htd1, etd1, hdzi, dzi, dz6, GG); break;
+            case 32: k_dpdtheta<T, 32><<<nbk, 128, 0, st>>>(n2, ncols, PS, SP, SPC, htd1, etd1, hdzi, dzi, dz6, GG); break;
             default: done = false;
         }
         if (done) {
@@ -1771,7 +2180,8 @@ struct Solver {
                 gprev = ((P(iz + 1) - P(iz - 1)) * hdzi - (1.0 / 6.0) * gprev) * htd1[iz - 1];
                 G(iz) = gprev;
             }
-            double gn = dz6 * (double)SP[cb + (size_t)nz * n2] - P(nz - 1) * dzi;
+            const double spn = (double)SP[cb + (size_t)nz * n2] + (SPC ? (double)SPC[cb + (size_t)nz * n2] : 0.0);
+            double gn = dz6 * spn - P(nz - 1) * dzi;
             gn = (gn - (1.0 / 3.0) * gprev) * htd1[nz - 1];
             G(nz) = gn;
             #pragma unroll 4
@@ -1807,10 +2217,13 @@ struct Solver {
         int sweeps = 0;
         int* hctl = reinterpret_cast<int*>(h_pinned);
         while (true) {
+            sweeps_run[refine32 ? host_kind : 0]++;
             psolve_sweep(nitmax, false, 0);
             sweeps++;
             SW_CUDA(cudaMemcpyAsync(hctl, ctrl.p, sizeof(int) * 3 * M, cudaMemcpyDeviceToHost, st));
+            if (refine32) SW_CUDA(cudaMemcpyAsync(hctl + 3 * M, sweep_kind.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             SW_CUDA(cudaStreamSynchronize(st));
+            if (refine32) host_kind = hctl[3 * M];
             bool any = false;
             for (int m = 0; m < M; m++) any = any || hctl[3 * m];
             if (!any || sweeps >= nitmax) break;
@@ -1838,8 +2251,14 @@ struct Solver {
         size_t nd = 0;
         SW_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
         require(cs == cudaStreamCaptureStatusActive, SW_ERR_STATE, "psolve_captured outside a capture");
-        cudaGraphConditionalHandle cond;
+        cudaGraphConditionalHandle cond, c64 = 0, c32 = 0;
         SW_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+        if (refine32) {
+            // the sweep bodies' IF conditions live in the step graph, so that every
+            // launch of the step starts each solve with a reference sweep
+            SW_CUDA(cudaGraphConditionalHandleCreate(&c64, g, 1, cudaGraphCondAssignDefault));
+            SW_CUDA(cudaGraphConditionalHandleCreate(&c32, g, 0, cudaGraphCondAssignDefault));
+        }
         cudaGraphNodeParams cp = {};
         cp.type = cudaGraphNodeTypeConditional;
         cp.conditional.handle = cond;
@@ -1853,8 +2272,9 @@ struct Solver {
         st = st_body;
         SW_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         const long long c0 = launch_counter().load();
-        psolve_sweep(nitmax, true, cond);
+        psolve_sweep(nitmax, true, cond, c64, c32);
         k_sweep = launch_counter().load() - c0;
+        if (!refine32) k_sweep_kind[0] = k_sweep;
         cudaGraph_t done;
         SW_CUDA(cudaStreamEndCapture(st, &done));
         st = outer;
@@ -2412,10 +2832,12 @@ struct Solver {
         long long* hx = reinterpret_cast<long long*>(h_pinned + 4);
         SW_CUDA(cudaMemcpyAsync(h, err_dev.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         SW_CUDA(cudaMemcpyAsync(h + 1, sweeps_dev.p, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
-        SW_CUDA(cudaMemcpyAsync(hx, sweep_exec.p, sizeof(long long), cudaMemcpyDeviceToHost, st));
-        SW_CUDA(cudaMemsetAsync(sweep_exec.p, 0, sizeof(long long), st));
+        SW_CUDA(cudaMemcpyAsync(hx, sweep_exec.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaMemsetAsync(sweep_exec.p, 0, 2 * sizeof(long long), st));
         SW_CUDA(cudaStreamSynchronize(st));
-        count_launch(fixed + hx[0] * k_sweep);
+        count_launch(fixed + hx[0] * k_sweep_kind[0] + hx[1] * k_sweep_kind[1]);
+        sweeps_run[0] += hx[0];
+        sweeps_run[1] += hx[1];
         for (int i = 0; i < 3; i++) last_sweeps[i] = h[1 + i];
         last_from_graph = true;
         if (h[0] != SW_OK) {

@@ -1,7 +1,7 @@
 """GPU tests of the batching and tuning layer: the float32 tile pass at n = 256,
 transform chunking, the chunk autotuner, asynchronous advance of several
-contexts, and 10-step parity of both precisions at ng=256, nz=16 against the
-FP64 oracle."""
+contexts, and 10-step parity of the three precisions at ng=256, nz=16 against
+the FP64 oracle."""
 import ctypes
 
 import numpy as np
@@ -34,7 +34,7 @@ def test_float32_transform_256_vs_oracle(sw, oracle):
     FP64 oracle's ptospc/spctop, per plane, forward and reverse: rel-L2 <= 1e-6
     (float32 rounding of inputs, twiddles and two radix-16 stages)."""
     ng, planes = 256, 34
-    sp = sw.Spectral(ng, 16, precision=sw.SW_MIXED)
+    sp = sw.Spectral(ng, 16, precision=sw.SW_FP32)
     osp = oracle.Spectral(ng, 4)
     rng = np.random.default_rng(11)
     x = rng.standard_normal(planes * ng * ng)
@@ -50,11 +50,19 @@ def test_float32_transform_256_vs_oracle(sw, oracle):
     assert rel_l2(p, xr) <= 2e-6
 
 
-@pytest.mark.parametrize("precision,ng", [(p, n) for p in ("fp64", "mixed") for n in (64, 256)])
+PRECISIONS = ("fp64", "mixed", "fp32")
+
+
+def _prec(sw, name):
+    return {"fp64": sw.SW_FP64, "mixed": sw.SW_MIXED, "fp32": sw.SW_FP32}[name]
+
+
+@pytest.mark.parametrize("precision,ng", [(p, n) for p in ("fp64", "fp32") for n in (64, 256)])
 def test_transform_chunk_does_not_change_results(sw, precision, ng):
     """Planes per launch pair and (at n = 256) columns per tile only change the
-    launch shape: bit-identical output."""
-    prec = sw.SW_FP64 if precision == "fp64" else sw.SW_MIXED
+    launch shape: bit-identical output (float64 transforms of SW_FP64 and SW_MIXED,
+    float32 of SW_FP32)."""
+    prec = _prec(sw, precision)
     dtype = np.float64 if precision == "fp64" else np.float32
     nz = 4
     sp = sw.Spectral(ng, nz, precision=prec, nmembers=2)
@@ -119,12 +127,12 @@ def test_autotune_reports_candidates_and_keeps_results(sw):
             assert np.array_equal(runs[0][m][k], runs[1][m][k]), (m, k)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", PRECISIONS)
 def test_async_advance_of_uneven_contexts_matches_sync(sw, precision):
     """Two contexts with different grids advanced with sw_advance_async and then
     sw_sync (running concurrently on their streams) give the fields of plain
     sw_advance, bit for bit, and the same sweep counts."""
-    prec = sw.SW_FP64 if precision == "fp64" else sw.SW_MIXED
+    prec = _prec(sw, precision)
     shapes = [(32, 4, 2), (48, 8, 1)]
     ref = []
     for ng, nz, M in shapes:
@@ -145,16 +153,27 @@ def test_async_advance_of_uneven_contexts_matches_sync(sw, precision):
         assert abs(_time(sw, sp) - 3.0 / ng) < 1e-15
 
 
-def test_ten_steps_256_both_precisions_vs_oracle(sw, oracle):
-    """ng=256, nz=16: 10 steps from vstrip + N(0,1e-3) q, both precisions against
-    the FP64 oracle.  delta and gamma (ds, gs) and the pressure are small residual
-    fields of cancelling terms; the gamma update amplifies any rounding difference
-    in q (a 1e-7 white-noise change of q moves gamma by ~4e-5 after one FP64 step
-    at ng=256, by ~1.5e-6 at ng=32).  So the FP64 path, which rounds differently
-    from the oracle's transforms, agrees to ~1e-15 on q, u, z and to ~1e-10 on
-    delta, gamma and p here; the mixed path's float32 rounding gives ~1e-7 on q
-    and ~1e-4 on delta and gamma (the 1e-5 mixed bound holds at ng=32, in
-    test_gpu_parity)."""
+# rel-L2 between two float64 oracle runs of this configuration that differ only in
+# the radix schedule of their transforms (tests/golden/oracle_spread.py 256 16 10):
+# the float64 rounding floor of the run, against which the FP64 path is judged.
+SPREAD_256 = {"qs": 1.19e-14, "u": 1.64e-14, "v": 1.00e-12, "z": 2.67e-15, "pn": 1.45e-11, "ds": 2.35e-10,
+              "gs": 9.59e-10}
+
+
+def test_ten_steps_256_all_precisions_vs_oracle(sw, oracle):
+    """ng=256, nz=16: 10 steps from vstrip + N(0,1e-3) q, each precision against
+    the FP64 oracle.
+
+    delta, gamma (ds, gs) and the pressure are small residual fields of cancelling
+    terms, and the gravity-wave part of the step amplifies rounding at high
+    wavenumbers, so their relative rounding error is the largest.
+    - SW_FP64: every field within 3x the oracle's own float64 spread (SPREAD_256).
+    - SW_MIXED: within the 1e-5 contract on every field (measured ~4e-8 on gamma:
+      float64 everywhere but the pressure sweeps, whose float32 corrections
+      converge to the 1e-7 stop rule).
+    - SW_FP32: its measured accuracy (float32 rounding of physical fields is white
+      and the k^2 factors of the gravity-wave terms amplify it: ~1e-4 on delta and
+      gamma).  That path does not meet 1e-5 at this size and does not claim it."""
     ng, nz, steps = 256, 16, 10
     qq = sw.vstrip.pv_strip(ng)
     rng = np.random.default_rng(1)
@@ -164,8 +183,10 @@ def test_ten_steps_256_both_precisions_vs_oracle(sw, oracle):
     for _ in range(steps):
         status, _, _ = oracle.advance(osp, ost, ggen=True)
         assert status == 0
-    bounds = {sw.SW_FP64: {"qs": 1e-12, "u": 1e-11, "z": 1e-12, "pn": 1e-9, "ds": 2e-9, "gs": 1e-8},
-              sw.SW_MIXED: {"qs": 1e-6, "u": 1e-5, "z": 1e-5, "pn": 1e-4, "ds": 1e-3, "gs": 3e-3}}
+    keys = ("qs", "u", "v", "z", "pn", "ds", "gs")
+    bounds = {sw.SW_FP64: {k: 3.0 * SPREAD_256[k] for k in keys},
+              sw.SW_MIXED: {k: 1e-5 for k in keys},
+              sw.SW_FP32: {"qs": 1e-6, "u": 1e-5, "v": 1e-5, "z": 1e-5, "pn": 1e-4, "ds": 1e-3, "gs": 3e-3}}
     errs = {}
     for prec, lim in bounds.items():
         sp = sw.Spectral(ng, nz, precision=prec)
@@ -177,7 +198,7 @@ def test_ten_steps_256_both_precisions_vs_oracle(sw, oracle):
     print("rel-L2 vs oracle after %d steps at ng=%d nz=%d: %s" % (steps, ng, nz, errs))
     for prec, lim in bounds.items():
         for k, tol in lim.items():
-            assert errs[prec][k] <= tol, "precision %d %s rel-L2 %.3e > %.0e" % (prec, k, errs[prec][k], tol)
+            assert errs[prec][k] <= tol, "precision %d %s rel-L2 %.3e > %.1e" % (prec, k, errs[prec][k], tol)
 
 
 def _thomas_numpy(a, b, c, d):
@@ -232,7 +253,7 @@ def test_async_state_copies_match_sync(sw):
     ng, nz, M = 32, 4, 2
     outs = []
     for asyn in (False, True):
-        sp = _ensemble(sw, ng, nz, M, sw.SW_MIXED, 90)
+        sp = _ensemble(sw, ng, nz, M, sw.SW_FP32, 90)
         L = sw._native.lib()
         n3 = sp.n3 * M
         fidx = sw._native.FIELD_INDEX
@@ -272,51 +293,52 @@ def _spec1d_numpy(ss, kmag, nb):
     return np.bincount(kmag.ravel(order="F"), weights=(w * ss * ss).ravel(order="F"), minlength=nb)[:nb]
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_savegrid_on_device_matches_host_composition(sw, precision):
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_savegrid_on_device_matches_oracle(sw, oracle, precision):
     """sw_savegrid (energies, shell spectra, float32 snapshots and 2-D fields in one
-    device call) against the same quantities composed on the host from the state
-    fields and the float64 transforms, as the reference's savegrid defines them
-    (src/nhswps/mod.rs:347-663)."""
-    prec = sw.SW_FP64 if precision == "fp64" else sw.SW_MIXED
+    device call) against the FP64 oracle's energy, spec1d and transforms applied to
+    the same state fields, as the reference's savegrid defines them
+    (src/nhswps/mod.rs:347-663).  The float32 outputs are compared at float32
+    rounding; the float32 work fields of SW_FP32 were themselves rounded."""
+    prec = _prec(sw, precision)
     ng, nz = 32, 4
+    L, n2 = nz + 1, ng * ng
     sp = _ensemble(sw, ng, nz, 1, prec, 55)
     sw._native.check(sw._native.lib().sw_advance(sp.ctx, 3, 1))
     st = sw.State.__new__(sw.State)
     object.__setattr__(st, "spectral", sp)
     object.__setattr__(st, "member", 0)
     energies, spec, f3, f2 = sw.nhswps.savegrid_data(st)
-    assert np.allclose(energies, sw.nhswps.energy(st), rtol=1e-13, atol=0)
-    f = {k: st.get(k) for k in ("qs", "ds", "gs", "r", "w", "pn", "z", "zeta")}
-    ref64 = sw.Spectral(ng, nz)  # float64 transforms as the host composition
-    nb = sp.kmax + 1
-    kmag = sp.kmag
-    weight = sp.weight
-    zs = sum(weight[iz] * _spec1d_numpy(ref64.ptospc(f["zeta"][:, :, iz]).reshape((ng, ng), order="F"), kmag, nb)
-             for iz in range(nz + 1))
-    ds = sum(weight[iz] * _spec1d_numpy(f["ds"][:, :, iz], kmag, nb) for iz in range(nz + 1))
-    gs = sum(weight[iz] * _spec1d_numpy(f["gs"][:, :, iz], kmag, nb) for iz in range(nz + 1))
-    spmf = sp.spmf[:nb]
-    tol = 1e-12 if precision == "fp64" else 1e-5
-    for got, ref in zip(spec, (zs * spmf, ds * spmf, gs * spmf)):
+    fields = {k: st.get(k).ravel(order="F") for k in sw._native.FIELDS}
+    osp = oracle.Spectral(ng, nz)
+    ost = oracle.State(ng, nz, fields)
+    assert np.allclose(energies, oracle.energy(osp, ost), rtol=1e-12, atol=0)
+    nb = int(osp.get("kmax")[0]) + 1
+    weight, spmf = osp.get("weight"), osp.get("spmf")[:nb]
+    lev = lambda a, iz: a[iz * n2:(iz + 1) * n2]
+    zs = sum(weight[iz] * osp.spec1d(osp.ptospc(lev(fields["zeta"], iz)))[:nb] for iz in range(L))
+    dsp = sum(weight[iz] * osp.spec1d(lev(fields["ds"], iz))[:nb] for iz in range(L))
+    gsp = sum(weight[iz] * osp.spec1d(lev(fields["gs"], iz))[:nb] for iz in range(L))
+    for got, ref in zip(spec, (zs * spmf, dsp * spmf, gsp * spmf)):
+        # zeta's spectrum comes from the device's own forward transform of zeta
+        tol = 1e-6 if precision == "fp32" else 1e-12
         assert np.abs(got - ref).max() <= tol * np.abs(ref).max()
-    L = nz + 1
+    phys = {k: osp.spctop3d(fields[k], np.zeros(L * n2), 0, nz) for k in ("qs", "ds", "gs")}
     for name in ("qs", "ds", "gs"):
-        phys = ref64.spctop3d(f[name], np.zeros((ng, ng, L), order="F"), 0, nz)
-        assert rel_l2(f3[name], phys) <= (1e-6 if precision == "fp64" else 2e-6), name
+        tol = 2e-6 if precision == "fp32" else 1e-7
+        assert rel_l2(f3[name], phys[name]) <= tol, name
     for name in ("r", "w", "pn"):
-        assert rel_l2(f3[name], f[name]) <= 1e-6, name
-    zt = f["z"][:, :, nz]
-    gphys = ref64.spctop3d(f["gs"], np.zeros((ng, ng, L), order="F"), 0, nz)
-    wz = sum(weight[iz] * f["zeta"][:, :, iz] * (1.0 + f["r"][:, :, iz]) for iz in range(L)) * 0.4 / zt
-    wg = sum(weight[iz] * gphys[:, :, iz] * (1.0 + f["r"][:, :, iz]) for iz in range(L)) * 0.4 / zt
+        assert rel_l2(f3[name], fields[name]) <= 1e-7, name
+    zt = lev(fields["z"], nz)
+    wz = sum(weight[iz] * lev(fields["zeta"], iz) * (1.0 + lev(fields["r"], iz)) for iz in range(L)) * 0.4 / zt
+    wg = sum(weight[iz] * lev(phys["gs"], iz) * (1.0 + lev(fields["r"], iz)) for iz in range(L)) * 0.4 / zt
     cof = 4.0 * np.pi
-    expect = {"d": -f["w"][:, :, nz] / zt, "zeta": wz, "q": 0.4 * (wz + cof) / zt - cof, "g": wg,
+    expect = {"d": -lev(fields["w"], nz) / zt, "zeta": wz, "q": 0.4 * (wz + cof) / zt - cof, "g": wg,
               "h": zt / 0.4 - 1.0}
     for name, ref in expect.items():
-        # gamma is a small residual field: its float32 transform in the mixed path
-        # carries a larger relative error than the others
-        tol = 1e-6 if precision == "fp64" else (1e-4 if name == "g" else 5e-6)
+        # gamma is a small residual field: in SW_FP32 its float32 transform carries a
+        # larger relative error than the others
+        tol = 1e-6 if precision != "fp32" else (1e-4 if name == "g" else 5e-6)
         assert rel_l2(f2[name], ref) <= tol, name
 
 

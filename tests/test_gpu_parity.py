@@ -3,8 +3,10 @@ vectors and the CPU oracle.
 
 Tolerances: the reference's own (1e-10 absolute for the spectral and nhswps
 functions, 1e-13 for transforms and slices, scaled by the fixture's magnitude
-where the reference compares bit-exactly), and rel-L2 <= 1e-12 against the FP64
-oracle for multi-step runs (the FP64 GPU path's stated tolerance).
+where the reference compares bit-exactly).  Multi-step runs against the FP64
+oracle: the FP64 path within 3x the oracle's own float64 rounding spread (the
+oracle run again with its second radix schedule, field by field); SW_MIXED within
+the 1e-5 rel-L2 of its contract; SW_FP32 within its measured, documented bounds.
 """
 import numpy as np
 import pytest
@@ -247,18 +249,93 @@ def _h(f, nz):
     return f[-f.size // (nz + 1):] / 0.4 - 1.0
 
 
+_SPREAD = {}
+
+
+def _config0_spread(oracle, steps):
+    """rel-L2 between two oracle runs of the configuration that differ only in the
+    radix schedule of their transforms: the float64 rounding floor of this run."""
+    if steps not in _SPREAD:
+        ng, nz = 32, 4
+        qq0 = oracle.vstrip(ng)
+        qb, _, _ = oracle.balinit(ng, nz, qq0)
+        rng = np.random.default_rng(1)
+        q3 = np.tile(qb, nz + 1) + rng.normal(0.0, 1.0e-3, ng * ng * (nz + 1))
+        z3 = np.zeros_like(q3)
+        runs = []
+        for order in (0, 1):
+            oracle.set_fft_order(order)
+            try:
+                osp, ost = oracle.initial_state(ng, nz, q3, z3, z3)
+                for _ in range(steps):
+                    assert oracle.advance(osp, ost, ggen=True)[0] == 0
+            finally:
+                oracle.set_fft_order(0)
+            runs.append(ost.f)
+        _SPREAD[steps] = {k: rel_l2(runs[1][k], runs[0][k]) for k in runs[0]}
+    return _SPREAD[steps]
+
+
 def test_fp64_ten_steps_vs_oracle(sw, oracle):
+    """The FP64 path after 10 steps against the oracle, every field within 3x the
+    oracle's own rounding spread (measured here: 9e-16 on qs, 8e-15 on u, 2e-12 on
+    pn, 3e-12 on delta, 5e-12 on gamma).  delta, gamma and p are small residual fields
+    whose relative rounding error is the largest."""
     st, ost = _config0(sw, oracle, sw.SW_FP64, 10)
+    spread = _config0_spread(oracle, 10)
     for k in ("qs", "ds", "gs", "u", "v", "z", "pn"):
         err = rel_l2(st.get(k), ost.f[k])
-        assert err <= 1e-11, "%s rel-L2 %.3e" % (k, err)
+        assert err <= 3.0 * max(spread[k], 1e-16), "%s rel-L2 %.3e > 3 x spread %.3e" % (k, err, spread[k])
 
 
 def test_mixed_ten_steps_vs_oracle(sw, oracle):
+    """SW_MIXED (float32 correction sweeps, stop rule 1e-7) within its 1e-5 rel-L2
+    contract on every field, the pressure included."""
     st, ost = _config0(sw, oracle, sw.SW_MIXED, 10)
-    for k in ("qs", "ds", "gs", "u", "v", "z"):
+    for k in ("qs", "ds", "gs", "u", "v", "z", "pn"):
         err = rel_l2(st.get(k), ost.f[k])
         assert err <= 1e-5, "%s rel-L2 %.3e" % (k, err)
+
+
+def test_fp32_ten_steps_vs_oracle(sw, oracle):
+    """SW_FP32 (float32 transforms and physical fields) at ng=32: within 1e-5 on
+    every field but the pressure, whose float32 iteration stops at 1e-6 or on
+    stagnation (bound 1e-4).  Its error grows with ng (test_gpu_batching, ng=256)."""
+    st, ost = _config0(sw, oracle, sw.SW_FP32, 10)
+    for k, tol in (("qs", 1e-5), ("ds", 1e-5), ("gs", 1e-5), ("u", 1e-5), ("v", 1e-5), ("z", 1e-5), ("pn", 1e-4)):
+        err = rel_l2(st.get(k), ost.f[k])
+        assert err <= tol, "%s rel-L2 %.3e > %.0e" % (k, err, tol)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "fp32"])
+def test_nonfinite_state_reports_diverged(sw, precision):
+    """A NaN put into qs from the host ends the pressure iteration with
+    SW_ERR_PSOLVE_DIVERGED (a deliberate deviation: the reference's `while errp >
+    toler` leaves the loop on a NaN as if converged, psolve.rs:88), in graph and
+    host-driven steps, and the context stays usable: a valid state then advances."""
+    import ctypes
+    prec = {"fp64": sw.SW_FP64, "mixed": sw.SW_MIXED, "fp32": sw.SW_FP32}[precision]
+    ng, nz = 32, 4
+    qq = sw.vstrip.pv_strip(ng)
+    rng = np.random.default_rng(4)
+    q3 = np.tile(qq, nz + 1) + rng.normal(0.0, 1.0e-3, ng * ng * (nz + 1))
+    z3 = np.zeros_like(q3)
+    L = sw._native.lib()
+    for graphs in (1, 0):
+        sp = sw.Spectral(ng, nz, precision=prec)
+        sw._native.check(L.sw_set_graphs(sp.ctx, graphs))
+        st = sw.nhswps.initial_state(sp, q3, z3, z3)
+        good = st.get("qs").copy()
+        bad = good.copy()
+        bad[3, 5, 2] = np.nan
+        st.set("qs", bad)
+        assert L.sw_advance(sp.ctx, 1, 1) == sw._native.SW_ERR_PSOLVE_DIVERGED
+        for k in FIELDS:  # a fresh state, as nhswps makes one (pressure first guess 0)
+            st.set(k, np.zeros(sp.n3))
+        st = sw.nhswps.initial_state(sp, q3, z3, z3)
+        sw._native.check(L.sw_advance(sp.ctx, 2, 1))
+        assert np.all(np.isfinite(st.get("gs")))
+        sp.close()
 
 
 def test_graph_steps_match_host_driven_steps(sw):
