@@ -111,6 +111,11 @@ int sw_ptospc3d(sw_ctx* ctx, const double* fp, double* fs, int izbeg, int izend)
 int sw_spctop3d(sw_ctx* ctx, const double* fs, double* fp, int izbeg, int izend);
 /* Spectral::spec1d (src/spectral/mod.rs:558-591): spec has ng+1 entries. */
 int sw_spec1d(sw_ctx* ctx, const double* ss, double* spec);
+/* balinit (src/balinit.rs:21-435): the balanced 2-D fields (qq, dd, gg; ng*ng each,
+ * Fortran order) of the PV field qq_init, by the reference's fixed-point iteration
+ * on the device.  *iters (may be NULL) gets the iteration count.  SW_FP64 and
+ * SW_MIXED contexts (float64); SW_ERR_STATE on SW_FP32. */
+int sw_balinit(sw_ctx* ctx, const double* qq_init, double* qq, double* dd, double* gg, int* iters);
 
 /* ---- nhswps numerics on the context's state (all members) ----------------------- */
 /* Spectral::main_invert (src/spectral/mod.rs:305-417): qs,ds,gs -> r,u,v,zeta. */
@@ -220,11 +225,17 @@ int sw_fft2d_dev(sw_ctx* ctx, int direction, int nplanes, const void* in, void* 
  * transform (a plugin inside a framework that owns the device memory pool, code
  * being captured into someone else's CUDA graph, allocation-free real-time loops).
  * in/out are the caller's device buffers of nplanes ng*ng planes (may alias);
- * stream is a cudaStream_t.  Scratch is a fixed 16 MiB array inside the library,
- * held by every GPU that loads it until exit; ng is limited to 1024 (larger sizes
- * return SW_ERR_ARG).  All calls share that array: calls overlapping on the GPU
- * race, so serialise them on one stream.  The first call on a device looks the
- * array's address up; make it before any stream capture that records this call. */
+ * stream is a cudaStream_t.  Scaling as sw_fft2d_dev and D2FFT: 1/sqrt(ng) per
+ * axis each way, so ptospc then spctop returns the input.  Scratch is a fixed
+ * 16 MiB array inside the library, held by every GPU that loads it until exit.
+ * Accepted: even ng in [4, 1024] that factors into 2, 3 and 5, direction 0 or 1,
+ * nplanes >= 1 and non-NULL buffers; otherwise SW_ERR_ARG (size, direction,
+ * buffers) or SW_ERR_FACTORISE (another prime factor).  A CUDA error pending from
+ * the caller's earlier work is reported as SW_ERR_CUDA and left pending.  All
+ * calls share the scratch array: calls overlapping on the GPU race, so serialise
+ * them on one stream.  The first call on a device (and the first after the
+ * device's context changes) looks the array's address up; make it before any
+ * stream capture that records this call. */
 int sw_fft2d_noalloc(int ng, int direction, int nplanes, const double* in, double* out, void* stream);
 /* Number of kernels the library launched on this context so far. */
 int sw_kernel_launches(sw_ctx* ctx, long long* count);

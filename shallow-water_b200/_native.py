@@ -56,6 +56,7 @@ _SIGS = {
     "sw_ptospc3d": (_i, [_vp, _dp, _dp, _i, _i]),
     "sw_spctop3d": (_i, [_vp, _dp, _dp, _i, _i]),
     "sw_spec1d": (_i, [_vp, _dp, _dp]),
+    "sw_balinit": (_i, [_vp, _dp, _dp, _dp, _dp, _ip]),
     "sw_main_invert": (_i, [_vp]),
     "sw_vertical": (_i, [_vp]),
     "sw_coeffs": (_i, [_vp, _dp, _dp, _dp, _dp]),

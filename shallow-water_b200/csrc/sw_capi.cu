@@ -498,6 +498,214 @@ int fft2d_impl(Solver<T>& s, int direction, int nplanes, const void* in, void* o
     return SW_OK;
 }
 
+
+// Reduction bodies of one plane for reduce_groups: f(i) -> one value, or RedVals<2>.
+template <class F>
+struct PlaneSum1 {
+    F f;
+    __device__ RedVals<1> operator()(int, long long i) const {
+        RedVals<1> r;
+        r.v[0] = f((int)i);
+        return r;
+    }
+};
+template <class F>
+struct PlaneSum2 {
+    F f;
+    __device__ RedVals<2> operator()(int, long long i) const { return f((int)i); }
+};
+
+// balinit (src/balinit.rs:21-435): the balanced 2-D initial fields of the PV strip,
+// as a fixed-point iteration over one ng x ng plane, entirely on the device: the
+// transforms, derivatives, products, filters and the scalar sums (deterministic
+// reductions into device scalars that the following kernels read).  The host reads
+// only the two relative changes per iteration for the stop test (toler 1e-9, or
+// the change stops falling).  float64 only.  Returns the iteration count.
+inline int balinit_impl(Solver<double>& s, const double* qin, double* qout, double* dout, double* gout) {
+    const int ng = s.ng, n2 = s.n2;
+    const double toler = 1.0E-9, small = 1.0E-12, dsumi = 1.0 / (double)(ng * ng);
+    cudaStream_t st = s.st;
+    const double *filt = s.op.filt, *opak = s.op.opak, *rlap = s.op.rlap, *helm = s.op.helm, *c2g2 = s.op.c2g2;
+    DevBuf<double> B((size_t)24 * n2), S(16);
+    double* const b = B.p;
+    double *QQ = b, *ZZ = b + n2, *UU = b + 2 * (size_t)n2, *VV = b + 3 * (size_t)n2, *HH = b + 4 * (size_t)n2;
+    double *DD = b + 5 * (size_t)n2, *GG = b + 6 * (size_t)n2, *DDP = b + 7 * (size_t)n2, *GGP = b + 8 * (size_t)n2;
+    double *DSs = b + 9 * (size_t)n2, *WA = b + 10 * (size_t)n2, *WB = b + 11 * (size_t)n2;
+    double *WP = b + 14 * (size_t)n2, *WQ = b + 15 * (size_t)n2;
+    // 8 planes: u, v spectra (0, 1) and their derivatives (4..7) for jacob; the
+    // physical products (0, 1) and their spectra (2, 3) for divs
+    double* X = b + 16 * (size_t)n2;
+    double* sc = S.p;  // 0 qadd, 1 qbar, 2 uio, 3 vio, 4..7 error sums
+    double* part = s.red_partial.p;
+    auto sum1 = [&](double* out, auto f) { reduce_groups<1>(st, 1, n2, 0u, PlaneSum1<decltype(f)>{f}, part, out); };
+    auto sum2 = [&](double* out, auto f) { reduce_groups<2>(st, 1, n2, 0u, PlaneSum2<decltype(f)>{f}, part, out); };
+    auto ptospc = [&](const double* src, double* dst) {
+        s.fft.ptospc(st, 1, [=] __device__(int, int iy, int ix) -> double { return src[iy + ng * ix]; },
+                     [=] __device__(int, int kx, int ky, double v) { dst[kx + ng * ky] = v; });
+    };
+    auto spctop = [&](const double* src, double* dst) {
+        s.fft.spctop(st, 1, [=] __device__(int, int kx, int ky) -> double { return src[kx + ng * ky]; },
+                     [=] __device__(int, int iy, int ix, double v) { dst[iy + ng * ix] = v; });
+    };
+    // divs(a, b) (src/spectral/mod.rs:461-475) of the physical products in X, X + n2
+    auto divs = [&](double* out) {
+        s.fft.ptospc(st, 2, [=] __device__(int o, int iy, int ix) -> double { return X[(size_t)o * n2 + iy + ng * ix]; },
+                     [=] __device__(int o, int kx, int ky, double v) { X[(size_t)(2 + o) * n2 + kx + ng * ky] = v; });
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            const int kx = i % ng, ky = i / ng;
+            out[i] = dmul(ky, ng) * X[3 * (size_t)n2 + kx + ng * mirror(ky, ng)] +
+                     dmul(kx, ng) * X[2 * (size_t)n2 + mirror(kx, ng) + ng * ky];
+        });
+    };
+    // the rlap, filter and velocity block shared by the set-up and the iteration:
+    // zz -> spectral, WA = rlap zz-hat, zz = filtered zz; u, v from WA (+ rlap ds)
+    auto velocity = [&](bool with_ds) {
+        ptospc(ZZ, WB);
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            WA[i] = rlap[i] * WB[i];
+            WB[i] = WB[i] * filt[i];
+        });
+        spctop(WB, ZZ);
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            const int kx = i % ng, ky = i / ng;
+            const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+            double u = -(dmul(ky, ng) * WA[my]), v = dmul(kx, ng) * WA[mx];  // -d/dy, d/dx of rlap zz
+            if (with_ds) {
+                u += dmul(kx, ng) * (rlap[mx] * DSs[mx]);
+                v += dmul(ky, ng) * (rlap[my] * DSs[my]);
+            }
+            WP[i] = u;
+            WQ[i] = v;
+        });
+        spctop(WP, UU);
+        spctop(WQ, VV);
+    };
+    SW_CUDA(cudaMemcpyAsync(QQ, qin, sizeof(double) * n2, cudaMemcpyHostToDevice, st));
+    SW_CUDA(cudaMemsetAsync(DD, 0, sizeof(double) * n2, st));
+    SW_CUDA(cudaMemsetAsync(GG, 0, sizeof(double) * n2, st));
+    SW_CUDA(cudaMemsetAsync(DDP, 0, sizeof(double) * n2, st));
+    SW_CUDA(cudaMemsetAsync(GGP, 0, sizeof(double) * n2, st));
+    // remove the mean of qq; hh from the inversion of f qq
+    sum1(sc + 0, [=] __device__(int i) { return QQ[i]; });
+    for_planes(st, 1, n2, [=] __device__(int, int i) { QQ[i] += -dsumi * sc[0]; });
+    sum1(sc + 1, [=] __device__(int i) { return QQ[i]; });
+    for_planes(st, 1, n2, [=] __device__(int, int i) { WP[i] = COF * QQ[i]; });
+    ptospc(WP, WB);
+    for_planes(st, 1, n2, [=] __device__(int, int i) { WA[i] = filt[i] * WB[i] / (opak[i] - COF * (dsumi * sc[1])); });
+    spctop(WA, HH);
+    sum1(sc + 0, [=] __device__(int i) { return (1.0 + HH[i]) * QQ[i]; });
+    for_planes(st, 1, n2, [=] __device__(int, int i) {
+        const double q = QQ[i] + (-dsumi * sc[0]);
+        QQ[i] = q;
+        ZZ[i] = (1.0 + HH[i]) * (COF + q) - COF;
+    });
+    velocity(false);
+    sum1(sc + 2, [=] __device__(int i) { return HH[i] * UU[i]; });
+    for_planes(st, 1, n2, [=] __device__(int, int i) { UU[i] += -sc[2] * dsumi; });
+    double* hs = s.h_pinned;
+    double toterrpre = 1.0 / (small * small), toterr = 0.5;
+    int iters = 0;
+    while (toterr > toler) {
+        iters++;
+        // gs = filt (div(dd u, dd v) - 2 J(u, v)); gg = spctop(gs).  J (src/spectral/
+        // mod.rs:423-453): u, v to spectral, their x, y derivatives back, u_x v_y - u_y v_x
+        s.fft.ptospc(st, 2, [=] __device__(int o, int iy, int ix) -> double {
+                         return (o ? VV : UU)[iy + ng * ix];
+                     },
+                     [=] __device__(int o, int kx, int ky, double v) { X[(size_t)o * n2 + kx + ng * ky] = v; });
+        s.fft.spctop(st, 4,
+            [=] __device__(int o, int kx, int ky) -> double {
+                const double* a = X + (size_t)(o / 2) * n2;
+                return (o & 1) ? dmul(ky, ng) * a[kx + ng * mirror(ky, ng)] : dmul(kx, ng) * a[mirror(kx, ng) + ng * ky];
+            },
+            [=] __device__(int o, int iy, int ix, double v) { X[(size_t)(4 + o) * n2 + iy + ng * ix] = v; });
+        s.fft.ptospc(st, 1,
+            [=] __device__(int, int iy, int ix) -> double {
+                const int i = iy + ng * ix;
+                const double* d = X + 4 * (size_t)n2;
+                return d[i] * d[3 * (size_t)n2 + i] - d[(size_t)n2 + i] * d[2 * (size_t)n2 + i];
+            },
+            [=] __device__(int, int kx, int ky, double v) { WB[kx + ng * ky] = v; });
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            X[i] = DD[i] * UU[i];
+            X[(size_t)n2 + i] = DD[i] * VV[i];
+        });
+        divs(WA);
+        for_planes(st, 1, n2, [=] __device__(int, int i) { WA[i] = filt[i] * (WA[i] - 2.0 * WB[i]); });
+        spctop(WA, GG);
+        sum2(sc + 4, [=] __device__(int i) {
+            RedVals<2> r;
+            const double e = GG[i] - GGP[i];
+            r.v[0] = e * e;
+            r.v[1] = GGP[i] * GGP[i];
+            return r;
+        });
+        // ds = helm (f div(zz u, zz v) - c2g2 div(hh u, hh v)); dd = spctop(ds)
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            X[i] = HH[i] * UU[i];
+            X[(size_t)n2 + i] = HH[i] * VV[i];
+        });
+        divs(WA);
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            X[i] = ZZ[i] * UU[i];
+            X[(size_t)n2 + i] = ZZ[i] * VV[i];
+        });
+        divs(WB);
+        for_planes(st, 1, n2, [=] __device__(int, int i) { DSs[i] = helm[i] * (COF * WB[i] - c2g2[i] * WA[i]); });
+        spctop(DSs, DD);
+        sum2(sc + 6, [=] __device__(int i) {
+            RedVals<2> r;
+            const double e = DD[i] - DDP[i];
+            r.v[0] = e * e;
+            r.v[1] = DDP[i] * DDP[i];
+            return r;
+        });
+        // hh from q and gamma; q's mean against htot; zz; u, v
+        sum1(sc + 0, [=] __device__(int i) { return QQ[i] * (1.0 + HH[i]); });
+        for_planes(st, 1, n2, [=] __device__(int, int i) { QQ[i] += -dsumi * sc[0]; });
+        sum1(sc + 1, [=] __device__(int i) { return QQ[i]; });
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            const double qbar = dsumi * sc[1];
+            WP[i] = COF * (QQ[i] + HH[i] * (QQ[i] - qbar)) - GG[i];
+        });
+        ptospc(WP, WB);
+        for_planes(st, 1, n2, [=] __device__(int, int i) { WA[i] = filt[i] * WB[i] / (opak[i] - COF * (dsumi * sc[1])); });
+        spctop(WA, HH);
+        sum1(sc + 0, [=] __device__(int i) { return QQ[i] * (1.0 + HH[i]); });
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            const double q = QQ[i] + (-dsumi * sc[0]);
+            QQ[i] = q;
+            ZZ[i] = (1.0 + HH[i]) * (COF + q) - COF;
+        });
+        velocity(true);
+        sum2(sc + 2, [=] __device__(int i) {
+            RedVals<2> r;
+            r.v[0] = HH[i] * UU[i];
+            r.v[1] = HH[i] * VV[i];
+            return r;
+        });
+        for_planes(st, 1, n2, [=] __device__(int, int i) {
+            UU[i] += -sc[2] * dsumi;
+            VV[i] += -sc[3] * dsumi;
+        });
+        SW_CUDA(cudaMemcpyAsync(hs, sc + 4, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+        SW_CUDA(cudaStreamSynchronize(st));
+        const double ggrmserr = hs[0] / (hs[1] + small), ddrmserr = hs[2] / (hs[3] + small);
+        toterr = 0.5 * (ddrmserr + ggrmserr);
+        if (toterrpre <= toterr) break;
+        SW_CUDA(cudaMemcpyAsync(DDP, DD, sizeof(double) * n2, cudaMemcpyDeviceToDevice, st));
+        SW_CUDA(cudaMemcpyAsync(GGP, GG, sizeof(double) * n2, cudaMemcpyDeviceToDevice, st));
+        toterrpre = toterr;
+        require(iters < 10000, SW_ERR_PSOLVE_MAXITER, "balinit did not converge");
+    }
+    for_planes(st, 1, n2, [=] __device__(int, int i) { WP[i] = ZZ[i] - COF * HH[i]; });
+    SW_CUDA(cudaMemcpyAsync(qout, WP, sizeof(double) * n2, cudaMemcpyDeviceToHost, st));
+    SW_CUDA(cudaMemcpyAsync(dout, DD, sizeof(double) * n2, cudaMemcpyDeviceToHost, st));
+    SW_CUDA(cudaMemcpyAsync(gout, GG, sizeof(double) * n2, cudaMemcpyDeviceToHost, st));
+    SW_CUDA(cudaStreamSynchronize(st));
+    return iters;
+}
+
 }  // namespace capi
 }  // namespace sw
 
@@ -534,6 +742,18 @@ int sw_spctop3d(sw_ctx* ctx, const double* fs, double* fp, int izbeg, int izend)
 }
 
 // spec1d (src/spectral/mod.rs:559-591): shell sums on the device, deterministic.
+// balinit (src/balinit.rs:21-435) on the context's device: float64 contexts only.
+int sw_balinit(sw_ctx* ctx, const double* qq_init, double* qq, double* dd, double* gg, int* iters) {
+    return guarded([&] {
+        require(ctx != nullptr && qq_init && qq && dd && gg, SW_ERR_ARG, "null argument");
+        require(ctx->s64 != nullptr, SW_ERR_STATE, "balinit runs on SW_FP64 and SW_MIXED contexts (float64)");
+        SW_CUDA(cudaSetDevice(ctx->device));
+        const int n = sw::capi::balinit_impl(*ctx->s64, qq_init, qq, dd, gg);
+        if (iters) *iters = n;
+        return SW_OK;
+    });
+}
+
 int sw_spec1d(sw_ctx* ctx, const double* ss, double* spec) {
     return with_solver(ctx, [&](auto& s) {
         require(ss && spec, SW_ERR_ARG, "null array");

@@ -127,6 +127,9 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
     const size_t smem = fft_pass_smem<T>(plan.n, tc);
     int dev = 0;
     cudaGetDevice(&dev);
+    // Kernel attributes are set once per device and kernel.  The flags are atomics
+    // because several host threads (one per context) may launch at once; two threads
+    // that both set an attribute set the same value, which is harmless.
     // compile-time pair kernels for the common lengths when the tile matches and
     // every tile is full (the generic kernel covers the rest)
     constexpr bool pair_ok = INV ? LCF : SCF;
@@ -134,11 +137,11 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
         if (plan.n == FFT_R_N && (tc == 16 || tc == 32) && ncols % tc == 0) {
             const int np = tc / 2;
             auto kern = np == 8 ? k_fft_pass_r<T, 8, INV, LCF, SCF, LD, ST> : k_fft_pass_r<T, 16, INV, LCF, SCF, LD, ST>;
-            static int attr_r[64][2] = {};
-            if (dev < 64 && !attr_r[dev][np == 8 ? 0 : 1]) {
+            static std::atomic<int> attr_r[64][2] = {};
+            if (dev < 64 && !attr_r[dev][np == 8 ? 0 : 1].load(std::memory_order_acquire)) {
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-                attr_r[dev][np == 8 ? 0 : 1] = 1;
+                attr_r[dev][np == 8 ? 0 : 1].store(1, std::memory_order_release);
             }
             dim3 grid(ncols / tc, nout);
             kern<<<grid, 16 * np, fft_pass_smem_r<T>(np), s>>>(tw, sc, ld, st);
@@ -151,11 +154,11 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
         // n = 128 (n = 256 tiles are all served by the register-staged pass above)
         if (plan.n == 128 && tc == (1 << LT128) && ncols % tc == 0) {
             auto kern = k_fft_pass_s<T, 128, LT128, INV, LCF, SCF, LD, ST>;
-            static int attr_s[64] = {};
-            if (dev < 64 && !attr_s[dev]) {
+            static std::atomic<int> attr_s[64] = {};
+            if (dev < 64 && !attr_s[dev].load(std::memory_order_acquire)) {
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
                 SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-                attr_s[dev] = 1;
+                attr_s[dev].store(1, std::memory_order_release);
             }
             dim3 grid(ncols / tc, nout);
             kern<<<grid, FFT_THREADS, smem, s>>>(tw, sc, ld, st);
@@ -165,11 +168,11 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
         }
     }
     auto kern = k_fft_pass<T, 0, 0, INV, LCF, SCF, LD, ST>;
-    static int attr_done[64] = {};
-    if (dev < 64 && !attr_done[dev]) {
+    static std::atomic<int> attr_done[64] = {};
+    if (dev < 64 && !attr_done[dev].load(std::memory_order_acquire)) {
         SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        attr_done[dev] = 1;
+        attr_done[dev].store(1, std::memory_order_release);
     }
     dim3 grid((ncols + tc - 1) / tc, nout);
     kern<<<grid, FFT_THREADS, smem, s>>>(plan, tw, ncols, ilog2(tc), make_fastdiv((uint32_t)plan.n), sc, ld, st);

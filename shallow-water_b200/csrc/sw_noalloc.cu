@@ -22,8 +22,12 @@
 //     streams, or from different host threads - race on it and give wrong results.
 //     Serialise such calls on one stream.
 //   * The first call on each device looks the array's device address up with
-//     cudaGetSymbolAddress (with that device current) and caches it; make that
-//     first call before any stream capture that includes this entry point.
+//     cudaGetSymbolAddress (with that device current) and caches it with the
+//     device's current CUDA context; make that first call before any stream capture
+//     that includes this entry point.  A call made under another context of the
+//     device (after a cudaDeviceReset, say) looks the address up again.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "sw_fft2d.cuh"
@@ -37,21 +41,42 @@ constexpr int MAX_NG = 1024;
 
 static __device__ __align__(256) unsigned char g_scratch[SCRATCH_BYTES];
 
-// Device address of g_scratch per device (host code cannot use the symbol itself).
+// Device address of g_scratch per device, with the context it was looked up in
+// (host code cannot use the symbol itself).
 static std::mutex g_mu;
 static void* g_addr[64] = {nullptr};
+static CUcontext g_ctx[64] = {nullptr};
+
+// The calling thread's current CUDA context, through the driver entry point that
+// the runtime hands out (no link against libcuda needed).
+static CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<Fn>(p);
+    }();
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 
 static int scratch_address(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return SW_ERR_CUDA;
     if (dev < 0 || dev >= 64) return SW_ERR_ARG;
+    const CUcontext ctx = current_context();
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    if (!g_addr[dev] || g_ctx[dev] != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess || p == nullptr) return SW_ERR_CUDA;
         g_addr[dev] = p;
+        g_ctx[dev] = current_context();  // the lookup may have made the primary context current
     }
     *out = g_addr[dev];
     return SW_OK;
@@ -114,6 +139,14 @@ static int run(int ng, int direction, int nplanes, const double* in, double* out
         msg = "sw_fft2d_noalloc: ng must factor into 2, 3 and 5";
         return SW_ERR_FACTORISE;
     }
+    // A launch error of this call must not be mixed up with an earlier error of the
+    // caller's own work: report a pending one as such and leave it in place.
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        msg = std::string("sw_fft2d_noalloc: a CUDA error was pending before the call: ") +
+              cudaGetErrorString(pending);
+        return SW_ERR_CUDA;
+    }
     void* base = nullptr;
     int st = scratch_address(&base);
     if (st != SW_OK) {
@@ -125,8 +158,9 @@ static int run(int ng, int direction, int nplanes, const double* in, double* out
     const size_t plane_bytes = (size_t)ng * ng * sizeof(double);
     const int cap = (int)((SCRATCH_BYTES - TWIDDLE_BYTES) / plane_bytes);
     k_twiddles<<<(ng + 255) / 256, 256, 0, s>>>(tw, ng);
-    if (cudaGetLastError() != cudaSuccess) {
-        msg = "sw_fft2d_noalloc: twiddle kernel launch failed";
+    const cudaError_t le = cudaGetLastError();  // nothing was pending, so this is the launch's own
+    if (le != cudaSuccess) {
+        msg = std::string("sw_fft2d_noalloc: twiddle kernel launch failed: ") + cudaGetErrorString(le);
         return SW_ERR_CUDA;
     }
     const int tc = pick_tile<double>(ng);

@@ -68,5 +68,6 @@ def pack(root, outdir):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    pack(ref, os.path.dirname(os.path.abspath(__file__)))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_CHECKOUT")
+    pack(sys.argv[1], os.path.dirname(os.path.abspath(__file__)))

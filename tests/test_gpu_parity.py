@@ -397,7 +397,27 @@ def test_ensemble_members_match_single_runs(sw):
             assert err <= 1e-12, "member %d %s rel-L2 %.3e" % (m, k, err)
 
 
-@pytest.mark.parametrize("ng,nz,dt,tsim", [(32, 4, 1.0 / 32, 1.0)])
+@pytest.mark.parametrize("ng,nz", [(18, 2), (32, 4)])
+def test_balinit_on_device_matches_golden(sw, ng, nz):
+    """sw_balinit (the fixed-point iteration on the device) against the
+    reference's sw_init.r8 of the same qq_init (src/balinit.rs:21-435), at the
+    oracle's tolerance for this fixture."""
+    g = golden("sta2dfft")
+    qq0 = g["balinit/%d_%d_qq_init.r8" % (ng, nz)][1:]
+    ref = g["balinit/%d_%d_sw_init.r8" % (ng, nz)].reshape(3, ng * ng + 1)[:, 1:]
+    got = sw.balinit.balance(ng, nz, qq0)
+    for a, b, name in zip(got, ref, ("qq", "dd", "gg")):
+        _close(a, b, 1e-11)
+
+
+def test_balinit_rejects_float32_context(sw):
+    sp = sw.Spectral(32, 4, precision=sw.SW_FP32)
+    with pytest.raises(sw.SwError) as e:
+        sw.balinit.balance(32, 4, np.zeros(32 * 32), spectral=sp)
+    assert e.value.status == sw._native.SW_ERR_STATE
+
+
+@pytest.mark.parametrize("ng,nz,dt,tsim", [(32, 4, 1.0 / 32, 1.0), (18, 4, 1.0 / 18, 2.0)])
 def test_nhswps_end_to_end(sw, tmp_path, ng, nz, dt, tsim):
     """vstrip -> balinit -> swto3d -> nhswps through the package (reference
     src/test.rs:29-40): monitor.asc and ecomp.asc match the reference's files to

@@ -170,3 +170,31 @@ def test_spec1d(oracle, ng, nz):
     ref = g[k + "spec2.bin"]
     kmax = int(oracle.Spectral(ng, nz).get("kmax")[0])
     _close(spec[: kmax + 1], ref[: kmax + 1], 1e-13)
+
+
+@pytest.mark.parametrize("n,s", FFT_CASES)
+def test_second_radix_schedule_matches_golden(oracle, n, s):
+    """The oracle's second radix schedule (5, 3, 2; the float64 floor of the GPU
+    tests comes from comparing the two schedules) computes the same transforms."""
+    g = golden("stafft")
+    oracle.set_fft_order(1)
+    try:
+        _rel(oracle.forfft(n, n, g["forfft/forfft_ng%d_%d_x.bin" % (n, s)]), g["forfft/forfft_ng%d_%d_x2.bin" % (n, s)])
+        _rel(oracle.revfft(n, n, g["revfft/revfft_ng%d_%d_x.bin" % (n, s)]), g["revfft/revfft_ng%d_%d_x2.bin" % (n, s)])
+    finally:
+        oracle.set_fft_order(0)
+    assert oracle.get_fft_order() == 0
+
+
+def test_radix_schedule_spread_is_float64_rounding(oracle):
+    """Two 3-step ng=32 runs under the two schedules differ at float64 rounding
+    only (delta, gamma and p most, being small residual fields)."""
+    import importlib.util
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "oracle_spread.py")
+    spec = importlib.util.spec_from_file_location("oracle_spread", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    sp = mod.spread(32, 4, 3)
+    assert all(0.0 < v < 1e-10 for v in sp.values()), sp
+    assert sp["qs"] < 1e-14
