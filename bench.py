@@ -10,8 +10,9 @@ is no dataset.  All fields (>= 8.9 MB each, ~0.5 GB working set) exceed the
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed|fp32]
     python bench.py --impl reference ...   (CPU FP64 oracle on the host cores)
 
-Multi-GPU (torchrun): one independent member per rank (replicas, weak scaling);
-the only collectives are the timing barrier and the max-over-ranks reduction.
+Multi-GPU: one ensemble per rank (replicas, weak scaling); the only collectives
+are the timing barrier and the max-over-ranks reduction.  Launched under torchrun,
+or as `python bench.py --gpus N`, which starts the N ranks itself.
 """
 import argparse
 import ctypes
@@ -628,6 +629,40 @@ def accuracy(sw, args, rank, local):
     return 0
 
 
+def free_port():
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def relaunch(n):
+    """`--gpus N` without a torchrun environment: start N ranks of this same command
+    line under torch.distributed.run (one process per GPU, rendezvous on 127.0.0.1)
+    and return their exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=%d" % n,
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def rank_check(args, rank, world):
+    """--rank-check: each rank joins a gloo process group (CPU) and rank 0 prints
+    the ranks and world size that the launch produced; no GPU work."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+    t = torch.tensor([rank], dtype=torch.int64)
+    got = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]
+    dist.all_gather(got, t)
+    if rank == 0:
+        print(json.dumps({"mode": "rank-check", "world_size": world, "gpus": args.gpus,
+                          "ranks": [int(g.item()) for g in got]}), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     global NG, NZ, METRIC
     ap = argparse.ArgumentParser()
@@ -666,6 +701,8 @@ def main():
     ap.add_argument("--autotune", default="on", choices=["on", "off"],
                     help="time the 2-D transform tile-width and launch-chunk candidates before warm-up and "
                          "keep the fastest")
+    ap.add_argument("--rank-check", action="store_true",
+                    help="only start the ranks (gloo, CPU) and print their ranks and world size")
     ap.add_argument("--graphs", default="on", choices=["on", "off"],
                     help="run each step as one CUDA graph (on) or host-driven (off; same kernels, for profiling)")
     args = ap.parse_args()
@@ -674,9 +711,13 @@ def main():
     if args.planes is None:
         args.planes = 6 * (NZ + 1)
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args.gpus)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.rank_check:
+        return rank_check(args, rank, world)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

@@ -48,3 +48,19 @@ def test_replicas_two_ranks():
     assert m0 == m1 == 2.0                 # max over ranks
     assert v0 == v1 == pytest.approx(2 * 3 / 2.0)
     assert q0 != q1                        # different seeds: independent members
+
+
+def test_bench_gpus_flag_starts_the_ranks():
+    """`python bench.py --gpus 2` with no torchrun environment starts two ranks
+    itself (torch.distributed.run on 127.0.0.1), each with its rank and the world
+    size; --rank-check keeps it to the launch (gloo, no GPU work)."""
+    import json
+    import subprocess
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                             "MASTER_PORT")}
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--rank-check"],
+                         env=env, capture_output=True, text=True, timeout=240)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    assert lines[0]["world_size"] == 2 and lines[0]["ranks"] == [0, 1]
