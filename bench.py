@@ -327,7 +327,7 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
         "tune": tune,
         "snapshot": {k: st.get(k).ravel(order="F") for k in ("qs", "ds", "gs", "pn")},
     }
-    if full:
+    if full and args.e2e == "on":
         n3 = sp.n3 * M
         fidx = sw._native.FIELD_INDEX
         pinned = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
@@ -353,6 +353,7 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
             pipe = e2e_pipelined(sw, L, args, M, prec, local, rank, tune, e2e_steps, world, barrier)
             res["e2e_sequential"] = res["e2e"]
             res["e2e"] = pipe
+    if full:
         res["fft"] = {"planes": fft_step[0], "per_launch_s": fft_step[1], "bytes": fft_step[2],
                       "one_member": {"planes": 6 * (NZ + 1), "per_launch_s": fft_pre[0], "bytes": fft_pre[1]}}
     sp.close()
@@ -375,6 +376,7 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
     for g in range(2):
         sp = sw.Spectral(NG, NZ, precision=prec, nmembers=half, device=local)
         if tune:
+            sw._native.check(L.sw_set_fft_overlap(sp.ctx, tune["overlap"], None))
             sp.set_fft_tile(tune["tile"])
             sp.set_fft_chunk(tune["chosen"])
         for j in range(half):
@@ -472,72 +474,61 @@ def drift(sw, args, rank, local):
 
 def uneven(sw, args, rank, world, local):
     """Ensemble of members with uneven grids: ng from {64, 96, 128, 192, 256}, nz
-    from {4, 8, 16}, drawn with a fixed seed.  Members of one (ng, nz) share one
-    batched context (one CUDA graph per step); the contexts' streams run
-    concurrently.  The timed region starts from one event that every context
-    stream waits on and ends when all of them have finished (CUDA events)."""
+    from {4, 8, 16}, drawn with a fixed seed, as one sw_ensemble: members of one
+    (ng, nz) share a batched context, and a step of every member is one CUDA graph
+    launch whose branches are the groups' steps.  Timed with CUDA events around the
+    queued steps on the ensemble's stream."""
     import torch
-    L = sw._native.lib()
     rng = np.random.default_rng(2024 + rank)
     draws = [(int(rng.choice([64, 96, 128, 192, 256])), int(rng.choice([4, 8, 16]))) for _ in range(args.uneven)]
+    prec = prec_code(sw, args.precision)
+    ens = sw.nhswps.Ensemble([d[0] for d in draws], [d[1] for d in draws], precision=prec, device=local)
+    strips = {}
+    for k, (ng, nz) in enumerate(draws):
+        if ng not in strips:
+            strips[ng] = sw.vstrip.pv_strip(ng)
+        q3, d3, g3 = initial_fields(ng, nz, 100 + k, lambda n: strips[ng])
+        ens.initial_state(k, q3, d3, g3)
+    ens.invert_all()
     groups = {}
     for k, key in enumerate(draws):
         groups.setdefault(key, []).append(k)
-    prec = prec_code(sw, args.precision)
-    ctxs = []
-    for (ng, nz), members in sorted(groups.items()):
-        sp = sw.Spectral(ng, nz, precision=prec, nmembers=len(members), device=local)
-        qq2 = sw.vstrip.pv_strip(ng)
-        for j, k in enumerate(members):
-            q3, d3, g3 = initial_fields(ng, nz, 100 + k, lambda n: qq2)
-            sw.nhswps.initial_state(sp, q3, d3, g3, member=j, invert=False)
-        sw.nhswps.main_invert_all(sp)
-        if args.autotune == "on":
-            sp.autotune()
-        sptr = ctypes.c_void_p()
-        sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(sptr)))
-        ctxs.append((ng, nz, len(members), sp, torch.cuda.ExternalStream(sptr.value)))
-    for sp in [c[3] for c in ctxs]:
-        sw._native.check(L.sw_advance_async(sp.ctx, args.warmup, 1))
-    for sp in [c[3] for c in ctxs]:
-        sw._native.check(L.sw_sync(sp.ctx))
+    if args.autotune == "on":
+        seen = set()
+        for k in range(len(draws)):
+            sp, _ = ens.member(k)
+            if id(sp) not in seen:
+                seen.add(id(sp))
+                sp.autotune()
+    ens.advance(args.warmup)  # the first step captures the combined graph
     torch.cuda.synchronize()
-    main = torch.cuda.current_stream()
+    es = torch.cuda.ExternalStream(ens.stream())
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        start.record(main)
-        ends = []
-        for ng, nz, cnt, sp, s in ctxs:
-            s.wait_event(start)
-            sw._native.check(L.sw_advance_async(sp.ctx, args.steps, 1))
-            e = torch.cuda.Event()
-            e.record(s)
-            ends.append(e)
-        for e in ends:
-            main.wait_event(e)
-        stop.record(main)
-        for sp in [c[3] for c in ctxs]:
-            sw._native.check(L.sw_sync(sp.ctx))
+        start.record(es)
+        ens.advance_async(args.steps)
+        stop.record(es)
+        ens.sync()
         torch.cuda.synchronize()
     secs = start.elapsed_time(stop) / 1e3
     secs = max_over_ranks(secs, world, "cuda")
-    points = sum(cnt * ng * ng * (nz + 1) for ng, nz, cnt, _, _ in ctxs)
+    points = sum(len(m) * ng * ng * (nz + 1) for (ng, nz), m in groups.items())
     if rank == 0:
         line = {
             "metric": "member-steps/s, uneven ensemble", "value": world * args.uneven * args.steps / secs,
             "unit": "member-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
-            "dtype": "f64" if prec == sw.SW_FP64 else "f32+f64", "data": "synthetic",
+            "dtype": {"fp64": "f64", "mixed": "f64+f32", "fp32": "f32+f64"}[args.precision], "data": "synthetic",
             "config": {"workload": "uneven ensemble: %d members, ng in {64,96,128,192,256}, nz in {4,8,16} "
-                                   "(seeded draw), vstrip + N(0,1e-3) q per member" % args.uneven,
-                       "groups": [{"ng": ng, "nz": nz, "members": cnt} for ng, nz, cnt, _, _ in ctxs],
+                                   "(seeded draw), vstrip + N(0,1e-3) q per member; one graph launch per step "
+                                   "of every member" % args.uneven,
+                       "groups": [{"ng": ng, "nz": nz, "members": len(m)} for (ng, nz), m in sorted(groups.items())],
                        "precision": args.precision},
             "grid_point_steps_per_s": world * points * args.steps / secs,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
-    for c in ctxs:
-        c[3].close()
+    ens.close()
     return 0
 
 
@@ -699,8 +690,12 @@ def main():
                     help="time an ensemble of MEMBERS members with ng drawn from {64,96,128,192,256} and nz "
                          "from {4,8,16}: one batched context per (ng, nz) group, groups run concurrently")
     ap.add_argument("--autotune", default="on", choices=["on", "off"],
-                    help="time the 2-D transform tile-width and launch-chunk candidates before warm-up and "
+                    help="time the 2-D transform tile-width, launch-chunk and two-stream pipeline candidates "
+                         "before warm-up and "
                          "keep the fastest")
+    ap.add_argument("--e2e", default="on", choices=["on", "off"],
+                    help="also measure the end-to-end loop through the C ABI with host buffers (off: for "
+                         "profiling runs)")
     ap.add_argument("--rank-check", action="store_true",
                     help="only start the ranks (gloo, CPU) and print their ranks and world size")
     ap.add_argument("--graphs", default="on", choices=["on", "off"],
@@ -794,7 +789,7 @@ def main():
                                           "fp32": "float32 transforms and work fields; not within 1e-5 on "
                                                   "delta/gamma at ng=256"}[args.precision],
                        "fft_autotune": main_arm["tune"]},
-            "e2e": main_arm["e2e"],
+            "e2e": main_arm.get("e2e"),
             "e2e_sequential": main_arm.get("e2e_sequential"),
             "gpu_launches": main_arm["launches"],
             "roofline": {"bound": "hbm", "kernel": "k_fft_pass_r (batched 2-D transform pass, %d planes per "

@@ -154,19 +154,37 @@ int sw_sweep_counts(sw_ctx* ctx, long long out[2]);
  * *in_use (may be NULL) gets the value now in use.  Results do not depend on it.  No reference counterpart:
  * the reference transforms one plane at a time (src/sta2dfft.rs:91-123). */
 int sw_set_fft_chunk(sw_ctx* ctx, int planes, int* in_use);
+/* Batched 2-D transforms at n = 256 as one single-pass launch (enable = 1):
+ * thread-block clusters of 8 CTAs each hold a plane and exchange its transposed
+ * intermediate through distributed shared memory, so every plane is read and
+ * written once.  enable = 0 (the default) selects the two tile passes through the
+ * intermediate in global memory; enable < 0 only queries.  *in_use (may be NULL) gets the
+ * setting in use (0 at other lengths).  Results are bit-identical.  No reference
+ * counterpart. */
+int sw_set_fft_single_pass(sw_ctx* ctx, int enable, int* in_use);
+/* Two-stream chunk pipeline of the batched 2-D transforms (enable = 1): chunks
+ * alternate between the context's stream and a second one with two intermediates,
+ * so that one chunk's second pass overlaps the next chunk's first pass and a chunk
+ * small enough keeps its intermediate in L2.  The chunk is then at most half the
+ * capacity.  enable = 0 (the default) runs the chunks in order on one stream;
+ * enable < 0 only queries.  *in_use (may be NULL) gets the setting.  Results are
+ * bit-identical.  No reference counterpart. */
+int sw_set_fft_overlap(sw_ctx* ctx, int enable, int* in_use);
 /* Columns per tile of the n = 256 tile passes, 16 or 32 (other lengths have a fixed
  * tile; columns <= 0 only queries).  *in_use (may be NULL) gets the value now in
  * use.  Results do not depend on it.  No reference counterpart. */
 int sw_set_fft_tile(sw_ctx* ctx, int columns, int* in_use);
-/* Autotuner of the tile width and the chunk: times reps forward + inverse
- * transforms of the pressure sweep's batch (3*nz planes per member) for each tile
- * width the grid has kernels for (n = 256: 16 and 32 columns) and each chunk (the
- * capacity, halved down to 8 planes), on scratch buffers it allocates, and keeps
- * the fastest pair.  Up to maxc rows of (tiles[i], chunks[i], ms[i] per transform
- * pair) are written when the arrays are non-NULL; *ncand gets the row count,
- * *chosen_tile and *chosen_chunk the values now in use.  No reference counterpart. */
-int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* tiles, int* chunks, float* ms, int* ncand, int* chosen_tile,
-                    int* chosen_chunk);
+/* Autotuner of the 2-D transform launches: times reps forward + inverse transforms
+ * of the pressure sweep's batch (3*nz planes per member) for each tile width the
+ * grid has kernels for (n = 256: 16 and 32 columns), each chunk (without the
+ * two-stream pipeline: the capacity halved down to 8 planes; with it: a half and a
+ * quarter of the capacity), on scratch buffers it allocates, and keeps the fastest.  Up
+ * to maxc rows of (tiles[i], chunks[i], overlaps[i], ms[i] per transform pair) are
+ * written when the arrays are non-NULL; *ncand gets the row count, *chosen_tile,
+ * *chosen_chunk and *chosen_overlap the values now in use.  No reference
+ * counterpart. */
+int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* tiles, int* chunks, int* overlaps, float* ms, int* ncand,
+                    int* chosen_tile, int* chosen_chunk, int* chosen_overlap);
 /* diagnose (src/nhswps/mod.rs:666-711) of one member:
  * out = {0.5*zrms^2, zrms, zmax, umax}. */
 int sw_diagnose(sw_ctx* ctx, int member, double out[4]);
@@ -237,6 +255,29 @@ int sw_fft2d_dev(sw_ctx* ctx, int direction, int nplanes, const void* in, void* 
  * device's context changes) looks the array's address up; make it before any
  * stream capture that records this call. */
 int sw_fft2d_noalloc(int ng, int direction, int nplanes, const double* in, double* out, void* stream);
+/* ---- ensembles of members with uneven grids ------------------------------------ */
+/* nmembers members, member k of grid ng[k] x ng[k] x (nz[k]+1), all of one
+ * precision on one device.  Members of one (ng, nz) share one batched context; a
+ * step of the whole ensemble is ONE CUDA graph launch whose parallel branches are
+ * the groups' steps, so the groups' kernels run concurrently.  The reference runs
+ * one member at a time and has no counterpart. */
+typedef struct sw_ensemble sw_ensemble;
+int sw_ensemble_create(const int* ng, const int* nz, int nmembers, int precision, int device, sw_ensemble** out);
+/* Destroys the ensemble and its group contexts. */
+void sw_ensemble_destroy(sw_ensemble* e);
+int sw_ensemble_info(const sw_ensemble* e, int* nmembers, int* ngroups);
+/* The stream the ensemble's step graphs are launched on (cudaStream_t as void*). */
+int sw_ensemble_stream(sw_ensemble* e, void** stream);
+/* The context that holds member `member` and the member's index in it: fields are
+ * set and read with the context's entry points (sw_state_set(ctx, field, index, ...)).
+ * The context belongs to the ensemble (do not destroy it); tune it (chunk, tile,
+ * tolerance) before the ensemble's first step, which captures the combined graph. */
+int sw_ensemble_member(sw_ensemble* e, int member, sw_ctx** ctx, int* index);
+/* nsteps steps of every member (ggen as sw_advance for the first); the _async form
+ * queues them and returns, sw_ensemble_sync waits and returns the worst status. */
+int sw_ensemble_advance(sw_ensemble* e, int nsteps, int ggen);
+int sw_ensemble_advance_async(sw_ensemble* e, int nsteps, int ggen);
+int sw_ensemble_sync(sw_ensemble* e);
 /* Number of kernels the library launched on this context so far. */
 int sw_kernel_launches(sw_ctx* ctx, long long* count);
 

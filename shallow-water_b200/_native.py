@@ -74,8 +74,10 @@ _SIGS = {
     "sw_state_get_all_async": (_i, [_vp, _i, _dp, _sz]),
     "sw_tridiag_batched": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "sw_tridiag_batched_host": (_i, [_i, _i, _dp, _dp, _dp, _dp, _dp]),
-    "sw_autotune_fft": (_i, [_vp, _i, _i, _ip, _ip, ctypes.POINTER(ctypes.c_float), _ip, _ip, _ip]),
+    "sw_autotune_fft": (_i, [_vp, _i, _i, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_float), _ip, _ip, _ip, _ip]),
     "sw_set_fft_tile": (_i, [_vp, _i, _ip]),
+    "sw_set_fft_single_pass": (_i, [_vp, _i, _ip]),
+    "sw_set_fft_overlap": (_i, [_vp, _i, _ip]),
     "sw_diagnose": (_i, [_vp, _i, _dp]),
     "sw_diag_history": (_i, [_vp, _dp, _i, _ip]),
     "sw_energy": (_i, [_vp, _i, _dp]),
@@ -86,6 +88,14 @@ _SIGS = {
     "sw_fft2d_dev": (_i, [_vp, _i, _i, _vp, _vp]),
     "sw_fft2d_noalloc": (_i, [_i, _i, _i, _vp, _vp, _vp]),
     "sw_kernel_launches": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "sw_ensemble_create": (_i, [_ip, _ip, _i, _i, _i, ctypes.POINTER(_vp)]),
+    "sw_ensemble_destroy": (None, [_vp]),
+    "sw_ensemble_info": (_i, [_vp, _ip, _ip]),
+    "sw_ensemble_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "sw_ensemble_member": (_i, [_vp, _i, ctypes.POINTER(_vp), _ip]),
+    "sw_ensemble_advance": (_i, [_vp, _i, _i]),
+    "sw_ensemble_advance_async": (_i, [_vp, _i, _i]),
+    "sw_ensemble_sync": (_i, [_vp]),
 }
 
 _lib = None

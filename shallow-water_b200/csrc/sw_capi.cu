@@ -948,6 +948,20 @@ int sw_sweep_counts(sw_ctx* ctx, long long out[2]) {
         return SW_OK;
     });
 }
+int sw_set_fft_single_pass(sw_ctx* ctx, int enable, int* in_use) {
+    return with_solver(ctx, [&](auto& s) {
+        const bool on = s.set_fft_single_pass(enable);
+        if (in_use) *in_use = on ? 1 : 0;
+        return SW_OK;
+    });
+}
+int sw_set_fft_overlap(sw_ctx* ctx, int enable, int* in_use) {
+    return with_solver(ctx, [&](auto& s) {
+        const bool on = s.set_fft_overlap(enable);
+        if (in_use) *in_use = on ? 1 : 0;
+        return SW_OK;
+    });
+}
 int sw_set_psolve_toler(sw_ctx* ctx, double toler) {
     return with_solver(ctx, [&](auto& s) {
         s.set_refine_toler(toler);
@@ -961,11 +975,11 @@ int sw_set_fft_chunk(sw_ctx* ctx, int planes, int* in_use) {
         return SW_OK;
     });
 }
-int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* tiles, int* chunks, float* ms, int* ncand, int* chosen_tile,
-                    int* chosen_chunk) {
+int sw_autotune_fft(sw_ctx* ctx, int reps, int maxc, int* tiles, int* chunks, int* overlaps, float* ms, int* ncand,
+                    int* chosen_tile, int* chosen_chunk, int* chosen_overlap) {
     if (maxc < 0) return fail(SW_ERR_ARG, "maxc must be >= 0");
     return with_solver(ctx, [&](auto& s) {
-        const int v = s.autotune_fft(reps, maxc, tiles, chunks, ms, ncand, chosen_tile);
+        const int v = s.autotune_fft(reps, maxc, tiles, chunks, overlaps, ms, ncand, chosen_tile, chosen_overlap);
         if (chosen_chunk) *chosen_chunk = v;
         return SW_OK;
     });
@@ -985,6 +999,180 @@ int sw_kernel_launches(sw_ctx* ctx, long long* count) {
     if (!count) return fail(SW_ERR_ARG, "null output");
     *count = launch_counter().load();
     return SW_OK;
+}
+
+}  // extern "C"
+
+// ---- ensembles of uneven grids ------------------------------------------------------
+// Members with different (ng, nz): one batched context per (ng, nz) group, and one
+// CUDA graph per step of the whole ensemble whose branches are the groups' steps
+// (captured from the groups' streams into one graph), so that a step of every
+// member is one graph launch and the groups' kernels run concurrently.
+struct sw_ensemble {
+    int device = 0, nmembers = 0;
+    std::vector<sw_ctx*> groups;
+    std::vector<std::pair<int, int>> where;  // member -> (group, index in the group)
+    cudaStream_t master = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    bool pending = false;
+    ~sw_ensemble() {
+        if (master) cudaStreamSynchronize(master);
+        for (auto& e : exec)
+            if (e) cudaGraphExecDestroy(e);
+        for (auto& j : joins)
+            if (j) cudaEventDestroy(j);
+        if (fork) cudaEventDestroy(fork);
+        if (master) cudaStreamDestroy(master);
+        for (auto* g : groups) sw_ctx_destroy(g);
+    }
+};
+
+namespace {
+
+template <class F>
+int each_solver(sw_ctx* c, F&& f) {
+    if (c->s64) return f(*c->s64);
+    return f(*c->s32);
+}
+
+cudaGraphExec_t ensemble_graph(sw_ensemble* e, bool ggen) {
+    cudaGraphExec_t& ex = e->exec[ggen ? 1 : 0];
+    if (ex) return ex;
+    SW_CUDA(cudaStreamBeginCapture(e->master, cudaStreamCaptureModeRelaxed));
+    try {
+        SW_CUDA(cudaEventRecord(e->fork, e->master));
+        for (size_t g = 0; g < e->groups.size(); g++) {
+            each_solver(e->groups[g], [&](auto& s) {
+                SW_CUDA(cudaStreamWaitEvent(s.st, e->fork, 0));
+                s.capture_step_body(ggen);
+                SW_CUDA(cudaEventRecord(e->joins[g], s.st));
+                return 0;
+            });
+            SW_CUDA(cudaStreamWaitEvent(e->master, e->joins[g], 0));
+        }
+    } catch (...) {
+        cudaGraph_t gr = nullptr;
+        cudaStreamEndCapture(e->master, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        throw;
+    }
+    cudaGraph_t gr;
+    SW_CUDA(cudaStreamEndCapture(e->master, &gr));
+    SW_CUDA(cudaGraphInstantiate(&ex, gr, 0));
+    SW_CUDA(cudaGraphDestroy(gr));
+    return ex;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw_ensemble_create(const int* ng, const int* nz, int nmembers, int precision, int device, sw_ensemble** out) {
+    return guarded([&] {
+        require(out && ng && nz && nmembers >= 1, SW_ERR_ARG, "bad ensemble arguments");
+        *out = nullptr;
+        std::map<std::pair<int, int>, std::vector<int>> by_grid;
+        for (int k = 0; k < nmembers; k++) by_grid[{ng[k], nz[k]}].push_back(k);
+        std::unique_ptr<sw_ensemble> e(new sw_ensemble());
+        e->device = device;
+        e->nmembers = nmembers;
+        e->where.resize(nmembers);
+        for (auto& kv : by_grid) {
+            sw_ctx* c = nullptr;
+            const int st = sw_ctx_create(kv.first.first, kv.first.second, (int)kv.second.size(), precision, device, &c);
+            if (st != SW_OK) return st;  // message already recorded
+            const int g = (int)e->groups.size();
+            e->groups.push_back(c);
+            for (size_t j = 0; j < kv.second.size(); j++) e->where[kv.second[j]] = {g, (int)j};
+        }
+        SW_CUDA(cudaSetDevice(device));
+        SW_CUDA(cudaStreamCreateWithFlags(&e->master, cudaStreamNonBlocking));
+        SW_CUDA(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+        e->joins.resize(e->groups.size(), nullptr);
+        for (auto& j : e->joins) SW_CUDA(cudaEventCreateWithFlags(&j, cudaEventDisableTiming));
+        *out = e.release();
+        return SW_OK;
+    });
+}
+
+void sw_ensemble_destroy(sw_ensemble* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    delete e;
+}
+
+int sw_ensemble_info(const sw_ensemble* e, int* nmembers, int* ngroups) {
+    if (!e) return fail(SW_ERR_ARG, "null ensemble");
+    if (nmembers) *nmembers = e->nmembers;
+    if (ngroups) *ngroups = (int)e->groups.size();
+    return SW_OK;
+}
+
+int sw_ensemble_stream(sw_ensemble* e, void** stream) {
+    if (!e || !stream) return fail(SW_ERR_ARG, "null argument");
+    *stream = (void*)e->master;
+    return SW_OK;
+}
+
+int sw_ensemble_member(sw_ensemble* e, int member, sw_ctx** ctx, int* index) {
+    if (!e || !ctx || member < 0 || member >= e->nmembers) return fail(SW_ERR_ARG, "bad member");
+    *ctx = e->groups[e->where[member].first];
+    if (index) *index = e->where[member].second;
+    return SW_OK;
+}
+
+int sw_ensemble_advance_async(sw_ensemble* e, int nsteps, int ggen) {
+    return guarded([&] {
+        require(e != nullptr && nsteps >= 0, SW_ERR_ARG, "bad ensemble advance arguments");
+        SW_CUDA(cudaSetDevice(e->device));
+        for (auto* c : e->groups)  // earlier work queued on a group's stream comes first
+            each_solver(c, [&](auto& s) {
+                require(s.use_graphs, SW_ERR_STATE, "ensemble steps need graphs on (sw_set_graphs)");
+                SW_CUDA(cudaEventRecord(e->fork, s.st));
+                SW_CUDA(cudaStreamWaitEvent(e->master, e->fork, 0));
+                return 0;
+            });
+        for (int k = 0; k < nsteps; k++) SW_CUDA(cudaGraphLaunch(ensemble_graph(e, k == 0 ? ggen != 0 : true), e->master));
+        for (auto* c : e->groups)
+            each_solver(c, [&](auto& s) {
+                s.note_external_steps(nsteps, ggen != 0);
+                return 0;
+            });
+        // later calls on a group's context are ordered after these steps
+        SW_CUDA(cudaEventRecord(e->fork, e->master));
+        for (auto* c : e->groups)
+            each_solver(c, [&](auto& s) {
+                SW_CUDA(cudaStreamWaitEvent(s.st, e->fork, 0));
+                return 0;
+            });
+        e->pending = true;
+        return SW_OK;
+    });
+}
+
+int sw_ensemble_sync(sw_ensemble* e) {
+    return guarded([&] {
+        require(e != nullptr, SW_ERR_ARG, "null ensemble");
+        SW_CUDA(cudaSetDevice(e->device));
+        SW_CUDA(cudaStreamSynchronize(e->master));
+        int worst = SW_OK;
+        for (auto* c : e->groups) {
+            const int st = each_solver(c, [&](auto& s) { return s.pending ? s.advance_finish() : SW_OK; });
+            if (st != SW_OK) worst = st;
+        }
+        e->pending = false;
+        if (worst == SW_ERR_PSOLVE_DIVERGED) return fail(worst, "Pressure error too large!");
+        if (worst == SW_ERR_PSOLVE_MAXITER) return fail(worst, "Exceeded maximum number of iterations to find pressure!");
+        return worst;
+    });
+}
+
+int sw_ensemble_advance(sw_ensemble* e, int nsteps, int ggen) {
+    const int st = sw_ensemble_advance_async(e, nsteps, ggen);
+    if (st != SW_OK) return st;
+    return sw_ensemble_sync(e);
 }
 
 }  // extern "C"

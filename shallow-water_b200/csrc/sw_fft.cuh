@@ -605,20 +605,27 @@ __device__ __forceinline__ void stage2_16x16(T2* v, const T2* __restrict__ tw4, 
     butterfly<16, INV>(v);
 }
 
-template <typename T, int NPT, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
-__global__ void __launch_bounds__(16 * NPT, fft_r_minb<T, NPT>())
-k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
+// Hooks of one register-staged tile (fft_r_tile): after_load() runs after the tile's
+// global loads are in registers and before its first shared-memory write;
+// before_store() runs after its last shared-memory read and before its first
+// store through st.  The plain pass needs neither; the single-pass cluster
+// transform (k_fft2d_cluster) uses them to share the tile buffer with the data it
+// exchanges between the CTAs of a cluster.
+struct NoHooks {
+    __device__ __forceinline__ void after_load() const {}
+    __device__ __forceinline__ void before_store() const {}
+};
+
+// One tile of the register-staged pass: plane o, columns c0 .. c0 + 2 NP - 1, all
+// 256 points; buf holds NP padded sequences, tw the 64 twiddles of stage2_16x16.
+template <typename T, int NPT, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST, class HK>
+__device__ __forceinline__ void fft_r_tile(const typename C2<T>::t* __restrict__ tw, typename C2<T>::t* buf, T sc,
+                                           const LD& ld, const ST& st, int o, int c0, const HK& hk) {
     using T2 = typename C2<T>::t;
     static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
     static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
-    constexpr int N = FFT_R_N, H = N / 2, NP = NPT, PL = FFT_R_PL, TC = 2 * NP;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T2* tw = reinterpret_cast<T2*>(smem_raw);  // 64 entries: the rows of stage2_16x16
-    T2* buf = tw + N;
+    constexpr int N = FFT_R_N, H = N / 2, NP = NPT, PL = FFT_R_PL;
     const int tid = threadIdx.x;
-    const int o = blockIdx.y;
-    const int c0 = blockIdx.x * TC;
-    if (tid < 64) tw[tid] = twg[(1 << (tid >> 4)) * (tid & 15)];
     // (pair, butterfly) with the pair index on the lanes (column-contiguous global
     // access) or the butterfly index on the lanes (point-contiguous access, and the
     // conflict-free order of the in-place shared-memory stage)
@@ -630,6 +637,7 @@ k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
         T2 v[16];
 #pragma unroll
         for (int r = 0; r < 16; r++) ld_pair<T>(ld, o, col, j + 16 * r, v[r].x, v[r].y);
+        hk.after_load();
         butterfly<16, false>(v);  // first stage: no twiddles
         T2* y = buf + p * PL;
 #pragma unroll
@@ -647,15 +655,22 @@ k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
         // unpack: modes k and n-k of both columns of pair p from Z[k], Z[n-k]
         const T2* z = buf + pl_ * PL;
         const int col2 = c0 + 2 * pl_;
+        T2 za[H / 16], zb[H / 16];
 #pragma unroll
         for (int u = 0; u < H / 16; u++) {
             const int k = jl + 16 * u;
+            za[u] = z[pad16(k)];
+            zb[u] = z[pad16(k == 0 ? H : N - k)];
+        }
+        hk.before_store();
+#pragma unroll
+        for (int u = 0; u < H / 16; u++) {
+            const int k = jl + 16 * u;
+            const T2 a = za[u], b = zb[u];
             if (k == 0) {
-                const T2 a = z[pad16(0)], b = z[pad16(H)];
                 st_pair<T>(st, o, col2, 0, a.x * sc, a.y * sc);
                 st_pair<T>(st, o, col2, H, b.x * sc, b.y * sc);
             } else {
-                const T2 a = z[pad16(k)], b = z[pad16(N - k)];
                 st_pair<T>(st, o, col2, k, T(0.5) * (a.x + b.x) * sc, T(0.5) * (a.y + b.y) * sc);
                 st_pair<T>(st, o, col2, N - k, T(0.5) * (a.y - b.y) * sc, T(0.5) * (b.x - a.x) * sc);
             }
@@ -672,6 +687,7 @@ k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
                 ld_pair<T>(ld, o, col, k, a1[u], b1[u]);
                 ld_pair<T>(ld, o, col, k == 0 ? H : N - k, a2[u], b2[u]);
             }
+            hk.after_load();
             T2* z = buf + pl_ * PL;
 #pragma unroll
             for (int u = 0; u < U; u++) {
@@ -707,10 +723,29 @@ k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
         const T2* z = buf + p * PL;
 #pragma unroll
         for (int r = 0; r < 16; r++) v[r] = z[pad16(k + 16 * r)];
+        hk.before_store();
         stage2_16x16<true>(v, tw, k);
 #pragma unroll
         for (int r = 0; r < 16; r++) st_pair<T>(st, o, col, k + 16 * r, v[r].x * sc, v[r].y * sc);
     }
+}
+
+// The 64 twiddles of stage2_16x16 (exp(-2 pi i m j / 256), m = 1, 2, 4, 8, j < 16)
+// from the length-256 table, into shared memory.
+template <typename T2>
+__device__ __forceinline__ void load_tw64(T2* tw, const T2* __restrict__ twg) {
+    if (threadIdx.x < 64) tw[threadIdx.x] = twg[(1 << (threadIdx.x >> 4)) * (threadIdx.x & 15)];
+}
+
+template <typename T, int NPT, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
+__global__ void __launch_bounds__(16 * NPT, fft_r_minb<T, NPT>())
+k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
+    using T2 = typename C2<T>::t;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* tw = reinterpret_cast<T2*>(smem_raw);  // 64 entries: the rows of stage2_16x16
+    T2* buf = tw + FFT_R_N;
+    load_tw64(tw, twg);
+    fft_r_tile<T, NPT, INV, LOAD_CF, STORE_CF>(tw, buf, sc, ld, st, blockIdx.y, blockIdx.x * 2 * NPT, NoHooks{});
 }
 
 }  // namespace sw

@@ -12,6 +12,8 @@
 //   ptospc: ld(o, iy, ix) -> T physical input,  st(o, kx, ky, T) spectral output
 // so products, derivatives, filters and combinations fuse into the passes.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "sw_core.cuh"
 
 namespace sw {
@@ -180,6 +182,146 @@ inline void launch_pass(cudaStream_t s, const FftPlan& plan, const typename C2<T
     count_launch();
 }
 
+// ---------------------------------------------------------------------------
+// Single-pass 2-D transform of n = 256 planes on thread-block clusters.
+//
+// A cluster of FFT2D_CL = 8 CTAs holds one plane: CTA r transforms columns
+// 32 r .. 32 r + 31 along the first axis (phase 1, the first pass of the two-pass
+// transform), leaving its 32 x 256 result in its own shared memory (E).  After a
+// cluster barrier, CTA r reads the 32 columns of the second axis that it owns
+// straight from the eight CTAs' E through distributed shared memory and
+// transforms them (phase 2, the second pass).  Each plane is read from and
+// written to global memory once; the transposed intermediate of the two-pass
+// transform never leaves the cluster.  E shares the tile buffer: phase 1 writes it
+// after its last read of the buffer (before_store), and phase 2 reuses the buffer
+// only after a second cluster barrier has seen every CTA's reads of E finish
+// (after_load).  Arithmetic and operation order per 1-D transform are those of the
+// register-staged pass, so results equal the two-pass transform's bit for bit.
+//   ptospc: phase 1 forward along ix for iy columns; E_r[kx][iy - 32 r];
+//           phase 2 forward along iy for kx columns
+//   spctop: phase 1 reverse along ky for kx columns; E_r[kx - 32 r][iy];
+//           phase 2 reverse along kx for iy columns
+// ---------------------------------------------------------------------------
+constexpr int FFT2D_CL = 8;                // CTAs per cluster (portable cluster size)
+constexpr int FFT2D_NP = FFT_R_N / FFT2D_CL / 2;  // column pairs per CTA (16: 256 threads)
+template <typename T>
+__host__ __device__ constexpr int fft2d_cl_minb() { return sizeof(T) == 8 ? 2 : 4; }
+template <typename T>
+inline size_t fft2d_cl_smem() {
+    return sizeof(typename C2<T>::t) * ((size_t)64 + (size_t)FFT2D_NP * FFT_R_PL);
+}
+
+// E of a forward transform: [kx (256)][iy - c0 (32)]
+template <typename T>
+struct ClFwdStore {  // phase 1: column iy (c0 .. c0+31), mode kx
+    using T2 = typename C2<T>::t;
+    static constexpr bool pair_io = true;
+    T* e;
+    int c0;
+    __device__ __forceinline__ void operator()(int, int c, int k, T v) const { e[k * 32 + (c - c0)] = v; }
+    __device__ __forceinline__ void st2(int, int c, int k, T a, T b) const {
+        T2 v;
+        v.x = a;
+        v.y = b;
+        *reinterpret_cast<T2*>(e + k * 32 + (c - c0)) = v;
+    }
+};
+template <typename T>
+struct ClFwdLoad {  // phase 2: column kx, point iy, from CTA iy / 32
+    using T2 = typename C2<T>::t;
+    static constexpr bool pair_io = true;
+    T* e;  // this CTA's E (mapped to the owner's with map_shared_rank)
+    __device__ __forceinline__ T operator()(int, int c, int j) const {
+        const T* src = cooperative_groups::this_cluster().map_shared_rank(e, (unsigned)(j >> 5));
+        return src[c * 32 + (j & 31)];
+    }
+    __device__ __forceinline__ T2 ld2(int, int c, int j) const {
+        const T* src = cooperative_groups::this_cluster().map_shared_rank(e, (unsigned)(j >> 5));
+        T2 v;
+        v.x = src[c * 32 + (j & 31)];
+        v.y = src[(c + 1) * 32 + (j & 31)];
+        return v;
+    }
+};
+// E of a reverse transform: [kx - c0 (32)][iy (256)]
+template <typename T>
+struct ClRevStore {  // phase 1: column kx (c0 .. c0+31), point iy
+    static constexpr bool pair_io = true;
+    T* e;
+    int c0;
+    __device__ __forceinline__ void operator()(int, int c, int p, T v) const { e[(c - c0) * 256 + p] = v; }
+    __device__ __forceinline__ void st2(int, int c, int p, T a, T b) const {
+        e[(c - c0) * 256 + p] = a;
+        e[(c + 1 - c0) * 256 + p] = b;
+    }
+};
+template <typename T>
+struct ClRevLoad {  // phase 2: column iy, point kx, from CTA kx / 32
+    using T2 = typename C2<T>::t;
+    static constexpr bool pair_io = true;
+    T* e;
+    __device__ __forceinline__ T operator()(int, int c, int p) const {
+        const T* src = cooperative_groups::this_cluster().map_shared_rank(e, (unsigned)(p >> 5));
+        return src[(p & 31) * 256 + c];
+    }
+    __device__ __forceinline__ T2 ld2(int, int c, int p) const {
+        const T* src = cooperative_groups::this_cluster().map_shared_rank(e, (unsigned)(p >> 5));
+        return *reinterpret_cast<const T2*>(src + (p & 31) * 256 + c);
+    }
+};
+// Phase 1 writes E into the tile buffer it has just read: all reads first.
+struct SyncBeforeStore {
+    __device__ __forceinline__ void after_load() const {}
+    __device__ __forceinline__ void before_store() const { __syncthreads(); }
+};
+// Phase 2 has read E of every CTA into registers: wait for the whole cluster
+// before the tile buffer (which is E) is written again.
+struct ClusterAfterLoad {
+    __device__ __forceinline__ void after_load() const { cooperative_groups::this_cluster().sync(); }
+    __device__ __forceinline__ void before_store() const {}
+};
+
+template <typename T, bool INV, class LD, class ST>
+__global__ void __cluster_dims__(FFT2D_CL, 1, 1) __launch_bounds__(16 * FFT2D_NP, fft2d_cl_minb<T>())
+k_fft2d_cluster(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
+    using T2 = typename C2<T>::t;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* tw = reinterpret_cast<T2*>(smem_raw);
+    T2* buf = tw + 64;
+    T* e = reinterpret_cast<T*>(buf);
+    const int r = (int)cooperative_groups::this_cluster().block_rank();
+    const int o = blockIdx.y, c0 = 32 * r;
+    load_tw64(tw, twg);
+    if constexpr (!INV) {
+        fft_r_tile<T, FFT2D_NP, false, true, true>(tw, buf, sc, ld, ClFwdStore<T>{e, c0}, o, c0, SyncBeforeStore{});
+        cooperative_groups::this_cluster().sync();
+        fft_r_tile<T, FFT2D_NP, false, false, true>(tw, buf, sc, ClFwdLoad<T>{e}, st, o, c0, ClusterAfterLoad{});
+    } else {
+        fft_r_tile<T, FFT2D_NP, true, true, false>(tw, buf, sc, ld, ClRevStore<T>{e, c0}, o, c0, SyncBeforeStore{});
+        cooperative_groups::this_cluster().sync();
+        fft_r_tile<T, FFT2D_NP, true, true, true>(tw, buf, sc, ClRevLoad<T>{e}, st, o, c0, ClusterAfterLoad{});
+    }
+}
+
+// nout planes of n = 256, one cluster of FFT2D_CL CTAs per plane.
+template <typename T, bool INV, class LD, class ST>
+inline void launch_fft2d_cluster(cudaStream_t s, const typename C2<T>::t* tw, T sc, int nout, LD ld, ST st) {
+    if (nout <= 0) return;
+    auto kern = k_fft2d_cluster<T, INV, LD, ST>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static std::atomic<int> attr[64] = {};
+    if (dev < 64 && !attr[dev].load(std::memory_order_acquire)) {
+        SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft2d_cl_smem<T>()));
+        SW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        attr[dev].store(1, std::memory_order_release);
+    }
+    dim3 grid(FFT2D_CL, nout);
+    kern<<<grid, 16 * FFT2D_NP, fft2d_cl_smem<T>(), s>>>(tw, sc, ld, st);
+    SW_CHECK_LAUNCH();
+    count_launch();
+}
+
 template <typename T>
 struct Fft2d {
     using T2 = typename C2<T>::t;
@@ -192,6 +334,31 @@ struct Fft2d {
     int chunk = 0;  // planes per pair of pass launches (<= cap)
     int tc = 2;
     T sc = 1;
+    // n = 256: one single-pass cluster launch per transform batch (k_fft2d_cluster)
+    // instead of two tile passes through the intermediate
+    bool single_pass = false;
+    // Two-stream chunk pipeline: chunks alternate between the caller's stream and
+    // s2 with two intermediates, so that one chunk's second pass overlaps the next
+    // chunk's first pass and small chunks keep their intermediate in L2.
+    bool overlap = false;
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    ~Fft2d() {
+        if (s2) cudaStreamDestroy(s2);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+    }
+    // On: needs the intermediate to hold two chunks (the chunk is clamped to cap/2).
+    bool set_overlap(bool on) {
+        if (on && !s2) {
+            SW_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+            SW_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+            SW_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        }
+        overlap = on && cap >= 2;
+        if (overlap && chunk > cap / 2) chunk = cap / 2;
+        return overlap;
+    }
 
     // Default chunk: the intermediate of one launch pair stays within about 40 MB,
     // a third of the 126 MB L2, so that pass B reads what pass A wrote from L2.
@@ -219,6 +386,12 @@ struct Fft2d {
         // n = 256: the register-staged pass (16- or 32-column tiles, one buffer)
         tc = ng == FFT_R_N ? 2 * fft_r_np<T>() : pick_tile<T>(ng);
         sc = (T)(1.0 / std::sqrt((double)ng));
+        single_pass = false;  // measured slower than the two passes so far; opt in with set_single_pass
+    }
+    // Single-pass transforms on (n = 256 only); returns the setting in use.
+    bool set_single_pass(bool on) {
+        single_pass = on && ng == FFT_R_N;
+        return single_pass;
     }
     // Columns per tile of the n = 256 passes: 16 or 32 (other lengths keep their
     // fixed tile); returns the value in use.
@@ -226,27 +399,67 @@ struct Fft2d {
         if (ng == FFT_R_N && (columns == 16 || columns == 32)) tc = columns;
         return tc;
     }
-    // Planes per launch pair, clamped to [1, cap]; returns the value in use.
+    // Planes per launch pair, clamped to [1, cap] (cap/2 with the two-stream
+    // pipeline); returns the value in use.
     int set_chunk(int planes) {
-        chunk = planes < 1 ? 1 : (planes > cap ? cap : planes);
+        const int mx = overlap ? cap / 2 : cap;
+        chunk = planes < 1 ? 1 : (planes > mx ? mx : planes);
         return chunk;
     }
 
     template <class LD, class ST>
     void spctop(cudaStream_t s, int nout, LD ld, ST st) const {
-        for (int o0 = 0; o0 < nout; o0 += chunk) {
-            const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
-            launch_pass<T, true, true, false>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidPC<T>{midp, ng});
-            launch_pass<T, true, true, true>(s, plan, tw.p, tc, sc, cnt, ng, MidCP<T>{midp, ng}, StOff<ST>{st, o0});
+        if (single_pass) {
+            launch_fft2d_cluster<T, true>(s, tw.p, sc, nout, ld, st);
+            return;
         }
+        const bool two = overlap && nout > chunk && can_fork(s);
+        if (two) fork(s);
+        for (int o0 = 0, k = 0; o0 < nout; o0 += chunk, k++) {
+            const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
+            cudaStream_t sk = (two && (k & 1)) ? s2 : s;
+            T* m = midp + ((two && (k & 1)) ? (size_t)chunk * ng * ng : 0);
+            launch_pass<T, true, true, false>(sk, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidPC<T>{m, ng});
+            launch_pass<T, true, true, true>(sk, plan, tw.p, tc, sc, cnt, ng, MidCP<T>{m, ng}, StOff<ST>{st, o0});
+        }
+        if (two) join(s);
+    }
+    // s2 can take chunks of work queued on s unless s2 already belongs to another
+    // stream capture than s's (it stays a member of a capture it joined until that
+    // capture ends, and a conditional node's body is captured as a capture of its
+    // own): then the chunks run on s alone.
+    bool can_fork(cudaStream_t s) const {
+        cudaStreamCaptureStatus a = cudaStreamCaptureStatusNone, b = cudaStreamCaptureStatusNone;
+        unsigned long long ia = 0, ib = 0;
+        SW_CUDA(cudaStreamGetCaptureInfo(s, &a, &ia));
+        SW_CUDA(cudaStreamGetCaptureInfo(s2, &b, &ib));
+        if (b == cudaStreamCaptureStatusNone) return true;
+        return a == cudaStreamCaptureStatusActive && ia == ib;
+    }
+    void fork(cudaStream_t s) const {
+        SW_CUDA(cudaEventRecord(ev_fork, s));
+        SW_CUDA(cudaStreamWaitEvent(s2, ev_fork, 0));
+    }
+    void join(cudaStream_t s) const {
+        SW_CUDA(cudaEventRecord(ev_join, s2));
+        SW_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
     }
     template <class LD, class ST>
     void ptospc(cudaStream_t s, int nout, LD ld, ST st) const {
-        for (int o0 = 0; o0 < nout; o0 += chunk) {
-            const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
-            launch_pass<T, false, true, true>(s, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidCP<T>{midp, ng});
-            launch_pass<T, false, false, true>(s, plan, tw.p, tc, sc, cnt, ng, MidPC<T>{midp, ng}, StOff<ST>{st, o0});
+        if (single_pass) {
+            launch_fft2d_cluster<T, false>(s, tw.p, sc, nout, ld, st);
+            return;
         }
+        const bool two = overlap && nout > chunk && can_fork(s);
+        if (two) fork(s);
+        for (int o0 = 0, k = 0; o0 < nout; o0 += chunk, k++) {
+            const int cnt = (nout - o0 < chunk) ? nout - o0 : chunk;
+            cudaStream_t sk = (two && (k & 1)) ? s2 : s;
+            T* m = midp + ((two && (k & 1)) ? (size_t)chunk * ng * ng : 0);
+            launch_pass<T, false, true, true>(sk, plan, tw.p, tc, sc, cnt, ng, LdOff<LD>{ld, o0}, MidCP<T>{m, ng});
+            launch_pass<T, false, false, true>(sk, plan, tw.p, tc, sc, cnt, ng, MidPC<T>{m, ng}, StOff<ST>{st, o0});
+        }
+        if (two) join(s);
     }
 };
 

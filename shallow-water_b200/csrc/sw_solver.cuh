@@ -738,6 +738,35 @@ struct Solver {
         return fft.set_chunk(planes);
     }
 
+    // Single-pass cluster transforms at n = 256 on or off (off by default); like the
+    // chunk, the captured step graphs hold the old launches, so they are dropped.
+    bool set_fft_single_pass(int enable) {
+        if (enable < 0 || (enable != 0) == fft.single_pass) return fft.single_pass;
+        SW_CUDA(cudaStreamSynchronize(st));
+        for (auto& e : step_exec)
+            if (e) {
+                SW_CUDA(cudaGraphExecDestroy(e));
+                e = nullptr;
+            }
+        if constexpr (sizeof(T) == 8) {
+            if (refine32) f32.set_single_pass(enable != 0);
+        }
+        return fft.set_single_pass(enable != 0);
+    }
+
+    // Two-stream chunk pipeline of the batched 2-D transforms on or off (enable < 0
+    // queries); like the chunk, the captured step graphs hold the old launches.
+    bool set_fft_overlap(int enable) {
+        if (enable < 0 || (enable != 0) == fft.overlap) return fft.overlap;
+        SW_CUDA(cudaStreamSynchronize(st));
+        for (auto& e : step_exec)
+            if (e) {
+                SW_CUDA(cudaGraphExecDestroy(e));
+                e = nullptr;
+            }
+        return fft.set_overlap(enable != 0);
+    }
+
     // Columns per tile of the n = 256 tile passes (16 or 32); like the chunk, the
     // captured step graphs hold the old launches, so they are dropped.
     int set_fft_tile(int columns) {
@@ -758,7 +787,8 @@ struct Solver {
     // context's stream, and keeps the fastest pair.  The batch runs on scratch
     // buffers allocated for the measurement.  Writes up to maxc (tile, chunk, ms
     // per transform pair) rows; returns the chosen chunk and sets *tile_out.
-    int autotune_fft(int reps, int maxc, int* tiles, int* cand, float* ms, int* ncand, int* tile_out) {
+    int autotune_fft(int reps, int maxc, int* tiles, int* cand, int* ovls, float* ms, int* ncand, int* tile_out,
+                     int* ovl_out) {
         if (reps < 1) reps = 1;
         const int nb = std::min(fft.cap, 3 * nz * M);
         DevBuf<T> a, b;
@@ -770,42 +800,59 @@ struct Solver {
         cudaEvent_t e0, e1;
         SW_CUDA(cudaEventCreate(&e0));
         SW_CUDA(cudaEventCreate(&e1));
-        std::vector<int> cands, tcs;
-        for (int c = fft.cap;; c /= 2) {
-            cands.push_back(c);
-            if (c / 2 < 8) break;
-        }
+        std::vector<int> tcs;
         if (ng == FFT_R_N) tcs = {16, 32};
         else tcs = {fft.tc};
-        int best = fft.chunk, best_tc = fft.tc, k = 0;
+        int best = fft.chunk, best_tc = fft.tc, best_ovl = fft.overlap ? 1 : 0, k = 0;
         float best_ms = 1e30f;
         try {
-            for (int tcv : tcs) {
-                set_fft_tile(tcv);
-                for (int c : cands) {
-                    set_fft_chunk(c);
-                    for (int r = -1; r < reps; r++) {  // r = -1: untimed warm-up
-                        if (r == 0) SW_CUDA(cudaEventRecord(e0, st));
-                        fft.ptospc(st, nb, [=] __device__(int o, int iy, int ix) -> T { return A[((size_t)o * ng + ix) * ng + iy]; },
-                                   [=] __device__(int o, int kx, int ky, T v) { B[((size_t)o * ng + ky) * ng + kx] = v; });
-                        fft.spctop(st, nb, [=] __device__(int o, int kx, int ky) -> T { return B[((size_t)o * ng + ky) * ng + kx]; },
-                                   [=] __device__(int o, int iy, int ix, T v) { A[((size_t)o * ng + ix) * ng + iy] = v; });
+            for (int ovl = 0; ovl < 2; ovl++) {
+                set_fft_overlap(ovl);
+                // chunks: the capacity halved down to 8 planes; with the pipeline, half and a
+                // quarter of the capacity only.  Smaller pipelined chunks win on the plain
+                // transform timed here (their intermediate stays in L2) but lose on whole
+                // steps, whose fused transforms read and write more fields per plane
+                // (measured at ng=256, 16 members: 51-plane chunks 2-3% slower per step
+                // than 408-plane chunks, which are 3-5% faster than no pipeline).
+                std::vector<int> cands;
+                if (ovl) {
+                    if (fft.cap / 2 >= 1) cands.push_back(fft.cap / 2);
+                    if (fft.cap / 4 >= 8) cands.push_back(fft.cap / 4);
+                } else {
+                    for (int c = fft.cap; c >= 1; c /= 2) {
+                        cands.push_back(c);
+                        if (c / 2 < 8) break;
                     }
-                    SW_CUDA(cudaEventRecord(e1, st));
-                    SW_CUDA(cudaEventSynchronize(e1));
-                    float t = 0.f;
-                    SW_CUDA(cudaEventElapsedTime(&t, e0, e1));
-                    t /= (float)reps;
-                    if (k < maxc) {
-                        if (tiles) tiles[k] = fft.tc;
-                        if (cand) cand[k] = fft.chunk;
-                        if (ms) ms[k] = t;
-                    }
-                    k++;
-                    if (t < best_ms) {
-                        best_ms = t;
-                        best = fft.chunk;
-                        best_tc = fft.tc;
+                }
+                for (int tcv : tcs) {
+                    set_fft_tile(tcv);
+                    for (int c : cands) {
+                        set_fft_chunk(c);
+                        for (int r = -1; r < reps; r++) {  // r = -1: untimed warm-up
+                            if (r == 0) SW_CUDA(cudaEventRecord(e0, st));
+                            fft.ptospc(st, nb, [=] __device__(int o, int iy, int ix) -> T { return A[((size_t)o * ng + ix) * ng + iy]; },
+                                       [=] __device__(int o, int kx, int ky, T v) { B[((size_t)o * ng + ky) * ng + kx] = v; });
+                            fft.spctop(st, nb, [=] __device__(int o, int kx, int ky) -> T { return B[((size_t)o * ng + ky) * ng + kx]; },
+                                       [=] __device__(int o, int iy, int ix, T v) { A[((size_t)o * ng + ix) * ng + iy] = v; });
+                        }
+                        SW_CUDA(cudaEventRecord(e1, st));
+                        SW_CUDA(cudaEventSynchronize(e1));
+                        float t = 0.f;
+                        SW_CUDA(cudaEventElapsedTime(&t, e0, e1));
+                        t /= (float)reps;
+                        if (k < maxc) {
+                            if (tiles) tiles[k] = fft.tc;
+                            if (cand) cand[k] = fft.chunk;
+                            if (ovls) ovls[k] = ovl;
+                            if (ms) ms[k] = t;
+                        }
+                        k++;
+                        if (t < best_ms) {
+                            best_ms = t;
+                            best = fft.chunk;
+                            best_tc = fft.tc;
+                            best_ovl = ovl;
+                        }
                     }
                 }
             }
@@ -817,6 +864,8 @@ struct Solver {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (ncand) *ncand = k < maxc ? k : maxc;
+        const int ovl_set = set_fft_overlap(best_ovl) ? 1 : 0;
+        if (ovl_out) *ovl_out = ovl_set;
         const int tc_set = set_fft_tile(best_tc);
         if (tile_out) *tile_out = tc_set;
         return set_fft_chunk(best);
@@ -2064,7 +2113,8 @@ struct Solver {
         T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
         if (refine32) fold_correction(true);
         const int n2z = 2 * nz;
-        const int mchunk = std::max(1, std::min(M, fft.chunk / n2z));
+        // the intermediate holds all members' 2 nz first-pass planes (cap = 6 (nz + 1) M)
+        const int mchunk = std::max(1, std::min(M, fft.cap / n2z));
         for (int m0 = 0; m0 < M; m0 += mchunk) {
             const int mc = std::min(mchunk, M - m0);
             launch_pass<T, true, true, false>(st, fft.plan, fft.tw.p, fft.tc, fft.sc, n2z * mc, ng,
@@ -2783,17 +2833,35 @@ struct Solver {
         }
     }
 
+    // The work of one step captured on st, which must be capturing already (into
+    // this context's step graph or into an ensemble's combined graph).  Records the
+    // kernels per step outside the sweep loops for the launch accounting.
+    void capture_step_body(bool ggen) {
+        const long long c0 = launch_counter().load();
+        advance_captured(ggen);
+        // nodes captured (nothing ran): kernels outside the sweep loops
+        const long long captured = launch_counter().load() - c0;
+        k_fixed[ggen ? 1 : 0] = captured - (ggen ? 3 : 2) * k_sweep;
+        launch_counter().fetch_sub(captured);
+    }
+
+    // Bookkeeping of nsteps steps launched by someone else's graph on another stream
+    // (an ensemble): time, pending status and launch accounting, as advance_enqueue.
+    void note_external_steps(int nsteps, bool ggen_first) {
+        for (int k = 0; k < nsteps; k++) {
+            const bool g = k == 0 ? ggen_first : true;
+            pending_fixed += k_fixed[g ? 1 : 0];
+            t += 1.0 / (double)ng;
+        }
+        pending = true;
+    }
+
     cudaGraphExec_t step_graph(bool ggen) {
         cudaGraphExec_t& ex = step_exec[ggen ? 1 : 0];
         if (!ex) {
             SW_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-            const long long c0 = launch_counter().load();
             try {
-                advance_captured(ggen);
-                // nodes captured (nothing ran): kernels outside the sweep loops
-                const long long captured = launch_counter().load() - c0;
-                k_fixed[ggen ? 1 : 0] = captured - (ggen ? 3 : 2) * k_sweep;
-                launch_counter().fetch_sub(captured);
+                capture_step_body(ggen);
             } catch (...) {
                 cudaGraph_t g;
                 cudaStreamEndCapture(st, &g);

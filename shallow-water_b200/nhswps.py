@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from ._native import FIELDS, FIELD_INDEX, SwError, check, dptr, lib
+from ._native import FIELDS, FIELD_INDEX, SW_FP64 as SW_FP64_DEFAULT, SwError, check, dptr, lib
 from .spectral import Spectral, flat, put
 
 HBAR = 0.4
@@ -316,6 +316,76 @@ def initial_state(spectral, qq, dd, gg, member=0, invert=True):
 def main_invert_all(spectral):
     """main_invert for every member of the context (src/spectral/mod.rs:305-417)."""
     check(lib().sw_main_invert(spectral.ctx))
+
+
+class Ensemble:
+    """Members with uneven grids advanced together (sw_ensemble_*): member k has
+    grid ngs[k] x ngs[k] x (nzs[k] + 1).  Members of one (ng, nz) share a batched
+    context; one step of every member is one CUDA graph launch whose branches are
+    the groups' steps.  ``state(k)`` is member k's State (fields read and written
+    through its context)."""
+
+    def __init__(self, ngs, nzs, precision=SW_FP64_DEFAULT, device=0):
+        ngs = (ctypes.c_int * len(ngs))(*[int(v) for v in ngs])
+        nzs = (ctypes.c_int * len(nzs))(*[int(v) for v in nzs])
+        h = ctypes.c_void_p()
+        check(lib().sw_ensemble_create(ngs, nzs, len(ngs), int(precision), int(device), ctypes.byref(h)))
+        self._h = h
+        self.nmembers = len(ngs)
+        self._spectral = {}
+
+    def member(self, k):
+        """(Spectral of the member's context, the member's index in it)."""
+        c, i = ctypes.c_void_p(), ctypes.c_int()
+        check(lib().sw_ensemble_member(self._h, int(k), ctypes.byref(c), ctypes.byref(i)))
+        if c.value not in self._spectral:
+            self._spectral[c.value] = Spectral.borrowed(c, self)
+        return self._spectral[c.value], i.value
+
+    def state(self, k):
+        sp, i = self.member(k)
+        st = State.__new__(State)
+        object.__setattr__(st, "spectral", sp)
+        object.__setattr__(st, "member", i)
+        return st
+
+    def initial_state(self, k, qq, dd, gg):
+        """Member k's start-up fields (as initial_state); call invert_all() after
+        loading every member."""
+        sp, i = self.member(k)
+        initial_state(sp, qq, dd, gg, member=i, invert=False)
+
+    def invert_all(self):
+        for sp in {id(v): v for v in self._spectral.values()}.values():
+            check(lib().sw_main_invert(sp.ctx))
+
+    def stream(self):
+        """The stream the ensemble's step graphs run on (an int cudaStream_t)."""
+        s = ctypes.c_void_p()
+        check(lib().sw_ensemble_stream(self._h, ctypes.byref(s)))
+        return s.value
+
+    def advance(self, nsteps=1, ggen=True):
+        check(lib().sw_ensemble_advance(self._h, int(nsteps), int(bool(ggen))))
+
+    def advance_async(self, nsteps=1, ggen=True):
+        check(lib().sw_ensemble_advance_async(self._h, int(nsteps), int(bool(ggen))))
+
+    def sync(self):
+        check(lib().sw_ensemble_sync(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            for sp in self._spectral.values():
+                sp._ctx = ctypes.c_void_p()
+            lib().sw_ensemble_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _read_r8(path):

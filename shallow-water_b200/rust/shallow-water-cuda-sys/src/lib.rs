@@ -13,6 +13,12 @@ pub struct SwCtx {
     _private: [u8; 0],
 }
 
+/// The opaque ensemble of members with uneven grids (sw_ensemble).
+#[repr(C)]
+pub struct SwEnsemble {
+    _private: [u8; 0],
+}
+
 pub const SW_OK: c_int = 0;
 pub const SW_ERR_FACTORISE: c_int = 1;
 pub const SW_ERR_CUDA: c_int = 2;
@@ -88,8 +94,10 @@ pub fn sw_last_error() -> *const c_char;
     pub fn sw_set_psolve_toler(ctx: *mut SwCtx, toler: c_double) -> c_int;
     pub fn sw_sweep_counts(ctx: *mut SwCtx, out: *mut c_longlong) -> c_int;
     pub fn sw_set_fft_chunk(ctx: *mut SwCtx, planes: c_int, in_use: *mut c_int) -> c_int;
+    pub fn sw_set_fft_single_pass(ctx: *mut SwCtx, enable: c_int, in_use: *mut c_int) -> c_int;
+    pub fn sw_set_fft_overlap(ctx: *mut SwCtx, enable: c_int, in_use: *mut c_int) -> c_int;
     pub fn sw_set_fft_tile(ctx: *mut SwCtx, columns: c_int, in_use: *mut c_int) -> c_int;
-    pub fn sw_autotune_fft(ctx: *mut SwCtx, reps: c_int, maxc: c_int, tiles: *mut c_int, chunks: *mut c_int, ms: *mut c_float, ncand: *mut c_int, chosen_tile: *mut c_int, chosen_chunk: *mut c_int) -> c_int;
+    pub fn sw_autotune_fft(ctx: *mut SwCtx, reps: c_int, maxc: c_int, tiles: *mut c_int, chunks: *mut c_int, overlaps: *mut c_int, ms: *mut c_float, ncand: *mut c_int, chosen_tile: *mut c_int, chosen_chunk: *mut c_int, chosen_overlap: *mut c_int) -> c_int;
     pub fn sw_diagnose(ctx: *mut SwCtx, member: c_int, out: *mut c_double) -> c_int;
     pub fn sw_diag_history(ctx: *mut SwCtx, out: *mut c_double, cap: c_int, count: *mut c_int) -> c_int;
     pub fn sw_energy(ctx: *mut SwCtx, member: c_int, out: *mut c_double) -> c_int;
@@ -103,5 +111,13 @@ pub fn sw_last_error() -> *const c_char;
     pub fn sw_stream(ctx: *mut SwCtx, stream: *mut *mut c_void) -> c_int;
     pub fn sw_fft2d_dev(ctx: *mut SwCtx, direction: c_int, nplanes: c_int, in_: *const c_void, out: *mut c_void) -> c_int;
     pub fn sw_fft2d_noalloc(ng: c_int, direction: c_int, nplanes: c_int, in_: *const c_double, out: *mut c_double, stream: *mut c_void) -> c_int;
+    pub fn sw_ensemble_create(ng: *const c_int, nz: *const c_int, nmembers: c_int, precision: c_int, device: c_int, out: *mut *mut SwEnsemble) -> c_int;
+    pub fn sw_ensemble_destroy(e: *mut SwEnsemble);
+    pub fn sw_ensemble_info(e: *const SwEnsemble, nmembers: *mut c_int, ngroups: *mut c_int) -> c_int;
+    pub fn sw_ensemble_stream(e: *mut SwEnsemble, stream: *mut *mut c_void) -> c_int;
+    pub fn sw_ensemble_member(e: *mut SwEnsemble, member: c_int, ctx: *mut *mut SwCtx, index: *mut c_int) -> c_int;
+    pub fn sw_ensemble_advance(e: *mut SwEnsemble, nsteps: c_int, ggen: c_int) -> c_int;
+    pub fn sw_ensemble_advance_async(e: *mut SwEnsemble, nsteps: c_int, ggen: c_int) -> c_int;
+    pub fn sw_ensemble_sync(e: *mut SwEnsemble) -> c_int;
     pub fn sw_kernel_launches(ctx: *mut SwCtx, count: *mut c_longlong) -> c_int;
 }

@@ -43,7 +43,22 @@ class Spectral:
         self._ctx = h
         self._cache = {}
 
+    @classmethod
+    def borrowed(cls, ctx, owner):
+        """A view of a context that `owner` (an Ensemble) created and destroys."""
+        self = cls.__new__(cls)
+        ng, nz, nm, pr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().sw_ctx_info(ctx, ctypes.byref(ng), ctypes.byref(nz), ctypes.byref(nm), ctypes.byref(pr)))
+        self.ng, self.nz, self.nmembers, self.precision = ng.value, nz.value, nm.value, pr.value
+        self._ctx = ctx
+        self._cache = {}
+        self._owner = owner
+        return self
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._ctx = ctypes.c_void_p()
+            return
         if getattr(self, "_ctx", None) and self._ctx.value:
             lib().sw_ctx_destroy(self._ctx)
             self._ctx = ctypes.c_void_p()
@@ -72,18 +87,20 @@ class Spectral:
         check(lib().sw_set_fft_tile(self._ctx, int(columns), ctypes.byref(v)))
         return v.value
 
-    def autotune(self, reps=5, maxc=32):
-        """Time the candidate tile widths and transform chunks on this context's
-        grid and keep the fastest.  Returns {"tile": columns, "chosen": planes,
-        "candidates": [(columns, planes, ms), ...]}."""
+    def autotune(self, reps=5, maxc=64):
+        """Time the candidate tile widths, transform chunks and the two-stream chunk
+        pipeline on this context's grid and keep the fastest.  Returns {"tile":
+        columns, "chosen": planes, "overlap": 0/1, "candidates": [(columns, planes,
+        overlap, ms), ...]}."""
         tiles = (ctypes.c_int * maxc)()
         chunks = (ctypes.c_int * maxc)()
+        ovls = (ctypes.c_int * maxc)()
         ms = (ctypes.c_float * maxc)()
-        n, tile, chosen = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        check(lib().sw_autotune_fft(self._ctx, int(reps), maxc, tiles, chunks, ms, ctypes.byref(n),
-                                    ctypes.byref(tile), ctypes.byref(chosen)))
-        return {"tile": tile.value, "chosen": chosen.value,
-                "candidates": [(tiles[i], chunks[i], float(ms[i])) for i in range(n.value)]}
+        n, tile, chosen, ovl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().sw_autotune_fft(self._ctx, int(reps), maxc, tiles, chunks, ovls, ms, ctypes.byref(n),
+                                    ctypes.byref(tile), ctypes.byref(chosen), ctypes.byref(ovl)))
+        return {"tile": tile.value, "chosen": chosen.value, "overlap": ovl.value,
+                "candidates": [(tiles[i], chunks[i], ovls[i], float(ms[i])) for i in range(n.value)]}
 
     @property
     def n2(self):

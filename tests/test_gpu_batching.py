@@ -59,9 +59,9 @@ def _prec(sw, name):
 
 @pytest.mark.parametrize("precision,ng", [(p, n) for p in ("fp64", "fp32") for n in (64, 256)])
 def test_transform_chunk_does_not_change_results(sw, precision, ng):
-    """Planes per launch pair and (at n = 256) columns per tile only change the
-    launch shape: bit-identical output (float64 transforms of SW_FP64 and SW_MIXED,
-    float32 of SW_FP32)."""
+    """Planes per launch pair, the two-stream chunk pipeline and (at n = 256)
+    columns per tile only change the launch shape: bit-identical output (float64
+    transforms of SW_FP64 and SW_MIXED, float32 of SW_FP32)."""
     prec = _prec(sw, precision)
     dtype = np.float64 if precision == "fp64" else np.float32
     nz = 4
@@ -69,15 +69,49 @@ def test_transform_chunk_does_not_change_results(sw, precision, ng):
     rng = np.random.default_rng(5)
     x = rng.standard_normal(40 * ng * ng)
     outs = []
-    for tile in ((16, 32) if ng == 256 else (0,)):
-        if tile:
-            assert sp.set_fft_tile(tile) == tile
-        for chunk in (1, 7, 10 ** 6):
-            used = sp.set_fft_chunk(chunk)
-            assert used >= 1
-            outs.append((_fft2d(sw, sp, 0, x, dtype), _fft2d(sw, sp, 1, x, dtype)))
+    L = sw._native.lib()
+    for ovl in (0, 1):
+        sw._native.check(L.sw_set_fft_overlap(sp.ctx, ovl, None))
+        for tile in ((16, 32) if ng == 256 else (0,)):
+            if tile:
+                assert sp.set_fft_tile(tile) == tile
+            for chunk in (1, 7, 10 ** 6):
+                used = sp.set_fft_chunk(chunk)
+                assert used >= 1
+                outs.append((_fft2d(sw, sp, 0, x, dtype), _fft2d(sw, sp, 1, x, dtype)))
     for o in outs[1:]:
         assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_single_pass_transform_matches_two_pass(sw, precision):
+    """The single-pass cluster transform at n = 256 (8 CTAs per plane, the
+    transposed intermediate exchanged through distributed shared memory) gives the
+    two tile passes' results bit for bit, both directions, and so does a step."""
+    prec = _prec(sw, precision)
+    dtype = np.float64 if precision == "fp64" else np.float32
+    ng, nz = 256, 4
+    sp = sw.Spectral(ng, nz, precision=prec, nmembers=2)
+    L = sw._native.lib()
+    on = ctypes.c_int()
+    rng = np.random.default_rng(6)
+    x = rng.standard_normal(37 * ng * ng)
+    outs = []
+    for single in (1, 0):
+        sw._native.check(L.sw_set_fft_single_pass(sp.ctx, single, ctypes.byref(on)))
+        assert on.value == single
+        outs.append((_fft2d(sw, sp, 0, x, dtype), _fft2d(sw, sp, 1, x, dtype)))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    sp.close()
+    fields = []
+    for single in (1, 0):
+        sp = _ensemble(sw, ng, nz, 1, prec, 17)
+        sw._native.check(L.sw_set_fft_single_pass(sp.ctx, single, None))
+        sw._native.check(L.sw_advance(sp.ctx, 2, 1))
+        fields.append(_fields(sw, sp, 1)[0])
+        sp.close()
+    for k in fields[0]:
+        assert np.array_equal(fields[0][k], fields[1][k]), k
 
 
 def _ensemble(sw, ng, nz, M, prec, seed0):
@@ -111,6 +145,27 @@ def _time(sw, sp):
     return t.value
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_two_stream_pipeline_in_graph_steps_matches(sw, precision):
+    """Steps captured into CUDA graphs with the two-stream chunk pipeline on (small
+    chunks, so that transforms fork onto the second stream, except inside the
+    pressure loop's conditional bodies) equal steps with it off, bit for bit."""
+    prec = _prec(sw, precision)
+    ng, nz, M = 64, 4, 2
+    L = sw._native.lib()
+    runs = []
+    for ovl in (0, 1):
+        sp = _ensemble(sw, ng, nz, M, prec, 61)
+        sw._native.check(L.sw_set_fft_overlap(sp.ctx, ovl, None))
+        sp.set_fft_chunk(3)
+        sw._native.check(L.sw_advance(sp.ctx, 3, 1))
+        runs.append(_fields(sw, sp, M))
+        sp.close()
+    for m in range(M):
+        for k in runs[0][m]:
+            assert np.array_equal(runs[0][m][k], runs[1][m][k]), (m, k)
+
+
 def test_autotune_reports_candidates_and_keeps_results(sw):
     ng, nz, M = 32, 4, 2
     runs = []
@@ -118,8 +173,10 @@ def test_autotune_reports_candidates_and_keeps_results(sw):
         sp = _ensemble(sw, ng, nz, M, sw.SW_FP64, 40)
         if tune:
             rep = sp.autotune(reps=2)
-            assert rep["candidates"] and (rep["tile"], rep["chosen"]) in [(t, c) for t, c, _ in rep["candidates"]]
-            assert all(ms > 0 for _, _, ms in rep["candidates"])
+            rows = rep["candidates"]
+            assert rows and (rep["tile"], rep["chosen"], rep["overlap"]) in [(t, c, o) for t, c, o, _ in rows]
+            assert all(ms > 0 for _, _, _, ms in rows)
+            assert {o for _, _, o, _ in rows} == {0, 1}
         sw._native.check(sw._native.lib().sw_advance(sp.ctx, 2, 1))
         runs.append(_fields(sw, sp, M))
     for m in range(M):
@@ -199,6 +256,34 @@ def test_ten_steps_256_all_precisions_vs_oracle(sw, oracle):
     for prec, lim in bounds.items():
         for k, tol in lim.items():
             assert errs[prec][k] <= tol, "precision %d %s rel-L2 %.3e > %.1e" % (prec, k, errs[prec][k], tol)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_uneven_ensemble_members_match_single_runs(sw, precision):
+    """sw_ensemble: members of uneven grids (three (ng, nz) groups) advanced by one
+    graph launch per step of every member match their single runs at 1e-12."""
+    prec = _prec(sw, precision)
+    draws = [(32, 4), (48, 8), (32, 4), (64, 4), (48, 8)]
+    ens = sw.nhswps.Ensemble([d[0] for d in draws], [d[1] for d in draws], precision=prec)
+    z = {}
+    for k, (ng, nz) in enumerate(draws):
+        qq = sw.vstrip.pv_strip(ng)
+        rng = np.random.default_rng(200 + k)
+        q3 = np.tile(qq, nz + 1) + rng.normal(0.0, 1.0e-3, ng * ng * (nz + 1))
+        z[k] = q3
+        ens.initial_state(k, q3, np.zeros_like(q3), np.zeros_like(q3))
+    ens.invert_all()
+    ens.advance(3)
+    got = {k: {f: ens.state(k).get(f) for f in ("qs", "ds", "gs", "pn")} for k in range(len(draws))}
+    ens.close()
+    for k, (ng, nz) in enumerate(draws):
+        sp = sw.Spectral(ng, nz, precision=prec)
+        st = sw.nhswps.initial_state(sp, z[k], np.zeros_like(z[k]), np.zeros_like(z[k]))
+        sw._native.check(sw._native.lib().sw_advance(sp.ctx, 3, 1))
+        for f in ("qs", "ds", "gs", "pn"):
+            err = rel_l2(got[k][f], st.get(f))
+            assert err <= 1e-12, "member %d %s rel-L2 %.3e" % (k, f, err)
+        sp.close()
 
 
 def _thomas_numpy(a, b, c, d):
