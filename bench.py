@@ -672,6 +672,8 @@ def main():
     ap.add_argument("--fft-only", action="store_true",
                     help="only time the batched 2-D transform pass (for profiling the top kernel)")
     ap.add_argument("--planes", type=int, default=None, help="planes of the --fft-only pass (default 6*(nz+1))")
+    ap.add_argument("--fft-single-pass", action="store_true",
+                    help="--fft-only: the single-pass cluster transform (n = 256) instead of the two tile passes")
     ap.add_argument("--fft-tile", type=int, default=0, choices=[0, 16, 32],
                     help="columns per tile of the --fft-only pass at ng=256 (0: the precision's default)")
     ap.add_argument("--ng", type=int, default=NG, help="horizontal grid (the headline workload is 256)")
@@ -730,6 +732,8 @@ def main():
         sp = sw.Spectral(NG, NZ, precision=prec, nmembers=nmem, device=local)
         if args.fft_tile:
             sp.set_fft_tile(args.fft_tile)
+        if args.fft_single_pass:
+            sw._native.check(sw._native.lib().sw_set_fft_single_pass(sp.ctx, 1, None))
         return fft_only(sw, sp, args, 4 if prec == sw.SW_FP32 else 8)
     if args.kernels:
         return kernels(sw, args, rank, local)

@@ -12,10 +12,22 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sw_cuda.h"
 #include "sw_fft.cuh"
 
 namespace sw {
+
+// NVTX range of one stage of the step (main_invert, psolve set-up, sweeps, source,
+// update), shown on a profiler's timeline for host-driven steps and graph captures.
+// NVTX is header-only and costs nothing when no tool is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ---- physical constants (reference src/constants.rs:8-17) -----------------
 constexpr double PI = 3.14159265358979323846;

@@ -561,13 +561,22 @@ constexpr int FFT_R_N = 256, FFT_R_PL = 256 + 16 + 1;
 // twice the registers (3% faster than 16 pairs at 2 CTAs per SM).
 template <typename T>
 __host__ __device__ constexpr int fft_r_np() { return sizeof(T) == 8 ? 8 : 16; }
-// CTAs per SM the launch bounds ask for (registers per thread <= 65536 / (16 NP MINB))
+// CTAs per SM the launch bounds ask for (registers per thread <= 65536 / (16 NP MINB)).
+// FP64 with 8 sequences per CTA: 5 (96 registers, a few spilled) measured 2-5 %
+// faster on B200 than 4 (126 registers, none spilled) and 6 (80 registers).
+#ifndef SW_FFT_R_MINB_F64
+#define SW_FFT_R_MINB_F64 5
+#endif
 template <typename T, int NP>
-__host__ __device__ constexpr int fft_r_minb() { return NP == 8 ? (sizeof(T) == 8 ? 4 : 8) : (sizeof(T) == 8 ? 2 : 4); }
+__host__ __device__ constexpr int fft_r_minb() {
+    return NP == 8 ? (sizeof(T) == 8 ? SW_FFT_R_MINB_F64 : 8) : (sizeof(T) == 8 ? 2 : 4);
+}
 
+// Shared memory of the register-staged pass: the 64 twiddles of stage2_16x16 and
+// NP padded sequences.
 template <typename T>
 inline size_t fft_pass_smem_r(int np) {
-    return sizeof(typename C2<T>::t) * ((size_t)FFT_R_N + (size_t)np * FFT_R_PL);
+    return sizeof(typename C2<T>::t) * ((size_t)64 + (size_t)np * FFT_R_PL);
 }
 
 // Second radix-16 stage of 256 = 16 x 16 on the slots j + 16 r of one sequence:
@@ -743,7 +752,7 @@ k_fft_pass_r(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
     using T2 = typename C2<T>::t;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* tw = reinterpret_cast<T2*>(smem_raw);  // 64 entries: the rows of stage2_16x16
-    T2* buf = tw + FFT_R_N;
+    T2* buf = tw + 64;
     load_tw64(tw, twg);
     fft_r_tile<T, NPT, INV, LOAD_CF, STORE_CF>(tw, buf, sc, ld, st, blockIdx.y, blockIdx.x * 2 * NPT, NoHooks{});
 }

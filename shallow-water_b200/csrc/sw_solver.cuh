@@ -892,6 +892,7 @@ struct Solver {
     // main_invert (src/spectral/mod.rs:305-417)
     // ======================================================================
     void main_invert() {
+        NvtxRange nv("main_invert");
         const int ng = this->ng, n2 = this->n2, L = this->L, ML = this->ML;
         const double *QS = qs, *DS = ds, *GS = gs, *rope = op.rope, *rlap = op.rlap, *wgt = op.weight;
         double* wkh = plane_d.p;
@@ -1455,6 +1456,7 @@ struct Solver {
     // which equals ptospc(w after it).  ux, uy, vx, vy are left in W(11..14) for
     // source() of the same stage (u, v do not change in between).
     void psolve_prepare_fused() {
+        NvtxRange nv("psolve_setup");
         const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
         const int Mnz = M * nz;
         const bool mixed = sizeof(T) == 4;
@@ -2108,6 +2110,7 @@ struct Solver {
     // current iterate ps + C, and its solve p1 stays in ps while correction sweeps
     // run; SP keeps the spectrum of S at the reference point p_ref.
     void sweep_reference() {
+        NvtxRange nv("psolve_sweep_float64");
         const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
         double* PS = ps;
         T *A = W(0), *B = W(1), *C = W(2), *D = W(3), *SP = W(4);
@@ -2145,6 +2148,7 @@ struct Solver {
     // to |p|, so the iteration converges well below float32 rounding of p while moving
     // about half the bytes of a float64 sweep.
     void sweep_correction() {
+        NvtxRange nv("psolve_sweep_float32_correction");
         if constexpr (sizeof(T) == 8) {
             const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
             const float *D1 = R32(9), *Cr = R32(10);
@@ -2192,6 +2196,7 @@ struct Solver {
 
     // pn and dp/dtheta after convergence (psolve.rs:367-410).
     void psolve_finish() {
+        NvtxRange nv("psolve_finish");
         const int ng = this->ng, n2 = this->n2, L = this->L, nz = this->nz, M = this->M, ML = this->ML;
         const double dz = HBAR / (double)nz, dzi = 1.0 / dz, dz6 = dz / 6.0;
         const double hdzi = (1.0 / 2.0) * (1.0 / (HBAR / (double)nz));
@@ -2345,6 +2350,7 @@ struct Solver {
     // plane_t: z derivatives at iz = 0.
     // ======================================================================
     void source(double* SQS, double* SDS, double* SGS, bool reuse_uv = false) {
+        NvtxRange nv("source");
         const int ng = this->ng, n2 = this->n2, L = this->L, M = this->M, ML = this->ML;
         const double *filt = op.filt, *hlap = op.hlap, *c2g2 = op.c2g2, *wgt = op.weight;
         const double *QS = qs, *DS = ds, *PSp = ps;
@@ -2684,6 +2690,7 @@ struct Solver {
     // WD(2..10): qsi, qsm, sqs, sds, nds, sgs, ngs, dsi, gsi
     // ======================================================================
     void advance_update(bool first) {
+        NvtxRange nv("advance_update");
         const int n2 = this->n2, L = this->L;
         const double dt = 1.0 / (double)ng, dt4 = dt / 4.0, dt4i = 1.0 / dt4;
         const double *diss = op.diss, *rdis = op.rdis, *fope = op.fope, *c2g2 = op.c2g2, *simp = op.simp,
@@ -2760,6 +2767,7 @@ struct Solver {
 
     // One step with host-driven pressure loops (one stream sync per sweep).
     int advance_direct(bool ggen) {
+        NvtxRange nv("advance_step");
         int it = 0;
         double e = 0.0;
         last_sweeps[0] = last_sweeps[1] = last_sweeps[2] = 0;
@@ -2812,6 +2820,7 @@ struct Solver {
     // solves iterate inside conditional WHILE nodes, so a step needs no host
     // round trip.
     void advance_captured(bool ggen) {
+        NvtxRange nv("advance_step_capture");
         SW_CUDA(cudaMemsetAsync(sweeps_dev.p, 0, sizeof(int) * 3 * M, st));
         StepHints hints(*this);
         if (ggen) {
