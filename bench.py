@@ -217,9 +217,11 @@ def replica_throughput(units_per_rank, t_local, world, device="cpu"):
     return world * units_per_rank / max_over_ranks(t_local, world, device)
 
 
-def time_fft_pass(sw, sp, planes, w_fft, reps=20):
+def time_fft_pass(sw, sp, planes, w_fft, reps=20, launches=2):
     """Average duration of one batched 2-D transform pass over `planes` planes,
-    CUDA events on the library's stream; returns (seconds per launch, bytes per launch)."""
+    CUDA events on the library's stream; returns (seconds per launch, bytes per launch).
+    `launches`: kernel launches per 2-D transform (2 tile passes, or 1 single-pass
+    cluster launch)."""
     import torch
     L = sw._native.lib()
     stream_ptr = ctypes.c_void_p()
@@ -240,16 +242,18 @@ def time_fft_pass(sw, sp, planes, w_fft, reps=20):
         sw._native.check(L.sw_fft2d_dev(sp.ctx, d, planes, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr())))
     k1.record(stream)
     torch.cuda.synchronize()
-    per_launch_s = k0.elapsed_time(k1) / 1e3 / (2 * reps)
+    per_launch_s = k0.elapsed_time(k1) / 1e3 / (launches * reps)
     return per_launch_s, 2 * planes * NG * NG * w_fft
 
 
 def fft_only(sw, sp, args, w_fft):
-    per, nbytes = time_fft_pass(sw, sp, args.planes, w_fft, reps=args.steps)
+    launches = 1 if args.fft_single_pass else 2
+    per, nbytes = time_fft_pass(sw, sp, args.planes, w_fft, reps=args.steps, launches=launches)
     peak, kind = measured_peak()
     print(json.dumps({"fft_pass_us": per * 1e6, "bytes_per_launch": nbytes, "gbs": nbytes / per / 1e9,
                       "frac": nbytes / per / 1e9 / peak, "planes": args.planes, "precision": args.precision,
-                      "tile": sp.set_fft_tile(0)}))
+                      "tile": sp.set_fft_tile(0), "launches_per_transform": launches,
+                      "transform_us": per * launches * 1e6}))
     return 0
 
 

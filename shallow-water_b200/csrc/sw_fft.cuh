@@ -625,8 +625,33 @@ struct NoHooks {
     __device__ __forceinline__ void before_store() const {}
 };
 
+// Lane layout of the pair-major phases of the register-staged pass.  Thread t
+// works on column pair t % NP and residue class cls(t / NP) of the 256 points
+// (points j, j + 16, ..., j + 240).  The real-pair pack and unpack combine point
+// k with point n - k, which lies in class 16 - j, so the classes are ordered
+// 0, 8, 1, 15, 2, 14, ..., 7, 9: classes j and 16 - j sit on lanes t and t ^ NP
+// of one warp (classes 0 and 8 pair with themselves) and exchange with shuffles.
+__device__ __forceinline__ int fft_r_class(int g) {
+    const int i = g >> 1;
+    return g < 2 ? 8 * g : ((g & 1) ? 16 - i : i);
+}
+template <typename T2>
+__device__ __forceinline__ T2 shfl_xor_c(T2 v, int m) {
+    T2 r;
+    r.x = __shfl_xor_sync(0xffffffffu, v.x, m);
+    r.y = __shfl_xor_sync(0xffffffffu, v.y, m);
+    return r;
+}
+
 // One tile of the register-staged pass: plane o, columns c0 .. c0 + 2 NP - 1, all
 // 256 points; buf holds NP padded sequences, tw the 64 twiddles of stage2_16x16.
+// 256 = 16 x 16: the first radix-16 stage runs on the 16 points of one residue
+// class in registers, one shared-memory transpose hands each thread the 16
+// first-stage outputs of one frequency class, and the second stage (twiddles and
+// radix 16) leaves that thread the modes k = j + 16 r of its class.  The forward
+// transform's unpack and the reverse transform's pack, which combine the complex
+// values at k and n - k of a column pair, swap eight values with the partner lane
+// (classes j and 16 - j) instead of going through shared memory again.
 template <typename T, int NPT, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST, class HK>
 __device__ __forceinline__ void fft_r_tile(const typename C2<T>::t* __restrict__ tw, typename C2<T>::t* buf, T sc,
                                            const LD& ld, const ST& st, int o, int c0, const HK& hk) {
@@ -634,15 +659,17 @@ __device__ __forceinline__ void fft_r_tile(const typename C2<T>::t* __restrict__
     static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
     static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
     constexpr int N = FFT_R_N, H = N / 2, NP = NPT, PL = FFT_R_PL;
+    static_assert(NP == 8 || NP == 16, "partner classes must share a warp");
     const int tid = threadIdx.x;
-    // (pair, butterfly) with the pair index on the lanes (column-contiguous global
-    // access) or the butterfly index on the lanes (point-contiguous access, and the
-    // conflict-free order of the in-place shared-memory stage)
-    const int pl_ = tid % NP, jl = tid / NP;  // pair-major
-    const int pp = tid / 16, jp = tid % 16;   // point-major
+    // pair-major (pair index on the lanes: column-contiguous global access) with the
+    // partner class order, and point-major (point index on the lanes: point-contiguous
+    // global access)
+    const int pl_ = tid % NP, jc = fft_r_class(tid / NP);
+    const int pp = tid / 16, jp = tid % 16;
+    const bool self0 = jc == 0, self8 = jc == 8;
 
     if constexpr (!INV) {
-        const int p = LOAD_CF ? pl_ : pp, j = LOAD_CF ? jl : jp, col = c0 + 2 * p;
+        const int p = LOAD_CF ? pl_ : pp, j = LOAD_CF ? jc : jp, col = c0 + 2 * p;
         T2 v[16];
 #pragma unroll
         for (int r = 0; r < 16; r++) ld_pair<T>(ld, o, col, j + 16 * r, v[r].x, v[r].y);
@@ -653,82 +680,77 @@ __device__ __forceinline__ void fft_r_tile(const typename C2<T>::t* __restrict__
         for (int r = 0; r < 16; r++) y[pad16(16 * j + r)] = v[r];
         __syncthreads();
         {
-            T2* z = buf + pp * PL;
+            const T2* z = buf + pl_ * PL;
 #pragma unroll
-            for (int r = 0; r < 16; r++) v[r] = z[pad16(jp + 16 * r)];
-            stage2_16x16<false>(v, tw, jp);
-#pragma unroll
-            for (int r = 0; r < 16; r++) z[pad16(jp + 16 * r)] = v[r];
-        }
-        __syncthreads();
-        // unpack: modes k and n-k of both columns of pair p from Z[k], Z[n-k]
-        const T2* z = buf + pl_ * PL;
-        const int col2 = c0 + 2 * pl_;
-        T2 za[H / 16], zb[H / 16];
-#pragma unroll
-        for (int u = 0; u < H / 16; u++) {
-            const int k = jl + 16 * u;
-            za[u] = z[pad16(k)];
-            zb[u] = z[pad16(k == 0 ? H : N - k)];
+            for (int r = 0; r < 16; r++) v[r] = z[pad16(jc + 16 * r)];
         }
         hk.before_store();
+        stage2_16x16<false>(v, tw, jc);
+        // unpack: v[s] = Z[k], k = jc + 16 s < n/2 (s < 8), with Z[n - k] from the
+        // partner's slot 15 - s (class 8: own slot 15 - s; class 0: own slot 16 - s,
+        // and modes 0 and n/2 from slots 0 and 8)
+        const int col2 = c0 + 2 * pl_;
+        const T hs = T(0.5) * sc;  // (a + b) hs == (0.5 (a + b)) sc exactly: scaling by 0.5 is exact
 #pragma unroll
-        for (int u = 0; u < H / 16; u++) {
-            const int k = jl + 16 * u;
-            const T2 a = za[u], b = zb[u];
-            if (k == 0) {
+        for (int s = 0; s < 8; s++) {
+            const T2 recv = shfl_xor_c(v[15 - s], NP);
+            const T2 a = v[s];
+            const T2 b = self0 ? v[s == 0 ? 8 : 16 - s] : (self8 ? v[15 - s] : recv);
+            const int k = jc + 16 * s;
+            if (s == 0 && self0) {
                 st_pair<T>(st, o, col2, 0, a.x * sc, a.y * sc);
                 st_pair<T>(st, o, col2, H, b.x * sc, b.y * sc);
             } else {
-                st_pair<T>(st, o, col2, k, T(0.5) * (a.x + b.x) * sc, T(0.5) * (a.y + b.y) * sc);
-                st_pair<T>(st, o, col2, N - k, T(0.5) * (a.y - b.y) * sc, T(0.5) * (b.x - a.x) * sc);
+                st_pair<T>(st, o, col2, k, (a.x + b.x) * hs, (a.y + b.y) * hs);
+                st_pair<T>(st, o, col2, N - k, (a.y - b.y) * hs, (b.x - a.x) * hs);
             }
         }
     } else {
-        // pack: points k and n-k of pair p (k = 0 takes 0 and n/2) into Z
-        {
-            constexpr int U = H / 16;
-            const int col = c0 + 2 * pl_;
-            T a1[U], b1[U], a2[U], b2[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int k = jl + 16 * u;
-                ld_pair<T>(ld, o, col, k, a1[u], b1[u]);
-                ld_pair<T>(ld, o, col, k == 0 ? H : N - k, a2[u], b2[u]);
-            }
-            hk.after_load();
-            T2* z = buf + pl_ * PL;
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const int k = jl + 16 * u;
-                T2 lo, hi;
-                if (k == 0) {
-                    lo.x = a1[u]; lo.y = b1[u];
-                    hi.x = a2[u]; hi.y = b2[u];
-                    z[pad16(0)] = lo;
-                    z[pad16(H)] = hi;
-                } else {
-                    lo.x = a1[u] - b2[u]; lo.y = a2[u] + b1[u];
-                    hi.x = a1[u] + b2[u]; hi.y = b1[u] - a2[u];
-                    z[pad16(k)] = lo;
-                    z[pad16(N - k)] = hi;
-                }
-            }
-        }
-        __syncthreads();
+        // pack: points k = jc + 16 s (s < 8) and n - k of pair pl_ (k = 0 takes 0 and
+        // n/2) give Z[k] (own slot s) and Z[n - k] (the partner's slot 15 - s; class
+        // 8: own slot 15 - s; class 0: own slot 16 - s, or 8 for n/2)
         T2 v[16];
         {
-            // first stage: slots j + 16 r in, 16 j + r out (all reads before any write)
-            T2* z = buf + pp * PL;
+            const int col = c0 + 2 * pl_;
+            T a1[8], b1[8], a2[8], b2[8];
 #pragma unroll
-            for (int r = 0; r < 16; r++) v[r] = z[pad16(jp + 16 * r)];
-            butterfly<16, true>(v);
-            __syncthreads();
+            for (int s = 0; s < 8; s++) {
+                const int k = jc + 16 * s;
+                ld_pair<T>(ld, o, col, k, a1[s], b1[s]);
+                ld_pair<T>(ld, o, col, k == 0 ? H : N - k, a2[s], b2[s]);
+            }
+            hk.after_load();
+            T2 hi0[8];
 #pragma unroll
-            for (int r = 0; r < 16; r++) z[pad16(16 * jp + r)] = v[r];
+            for (int s = 0; s < 8; s++) {
+                T2 lo, hi;
+                if (s == 0 && self0) {
+                    lo.x = a1[s]; lo.y = b1[s];
+                    hi.x = a2[s]; hi.y = b2[s];
+                } else {
+                    lo.x = a1[s] - b2[s]; lo.y = a2[s] + b1[s];
+                    hi.x = a1[s] + b2[s]; hi.y = b1[s] - a2[s];
+                }
+                const T2 recv = shfl_xor_c(hi, NP);
+                v[s] = lo;
+                v[15 - s] = self8 ? hi : recv;
+                hi0[s] = hi;
+            }
+            if (self0) {
+                v[8] = hi0[0];
+#pragma unroll
+                for (int s = 1; s < 8; s++) v[16 - s] = hi0[s];
+            }
+        }
+        // first stage on class jc: slots jc + 16 r in, 16 jc + r out
+        butterfly<16, true>(v);
+        {
+            T2* y = buf + pl_ * PL;
+#pragma unroll
+            for (int r = 0; r < 16; r++) y[pad16(16 * jc + r)] = v[r];
         }
         __syncthreads();
-        const int p = STORE_CF ? pl_ : pp, k = STORE_CF ? jl : jp, col = c0 + 2 * p;
+        const int p = STORE_CF ? pl_ : pp, k = STORE_CF ? jc : jp, col = c0 + 2 * p;
         const T2* z = buf + p * PL;
 #pragma unroll
         for (int r = 0; r < 16; r++) v[r] = z[pad16(k + 16 * r)];
