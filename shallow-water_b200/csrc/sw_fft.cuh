@@ -283,6 +283,137 @@ __device__ T2* smem_fft(const FftPlan& plan, T2* a, T2* b, const T2* tw, int np,
 }
 
 // Shared memory bytes of one pass: twiddles (n) + two tiles (tc/2 * n each).
+// Functors that tag `static constexpr bool pair_io = true` provide
+// ld2(o, col, pt) -> T2 and st2(o, col, pt, a, b) for the adjacent columns
+// (col, col+1), col even; others get two scalar calls.
+template <class F, class = void>
+struct pair_io : std::false_type {};
+template <class F>
+struct pair_io<F, std::void_t<decltype(F::pair_io)>> : std::integral_constant<bool, F::pair_io> {};
+
+template <typename T, class LD>
+__device__ __forceinline__ void ld_pair(const LD& ld, int o, int col, int j, T& a, T& b) {
+    if constexpr (pair_io<LD>::value) {
+        const auto v = ld.ld2(o, col, j);
+        a = v.x;
+        b = v.y;
+    } else {
+        a = (T)ld(o, col, j);
+        b = (T)ld(o, col + 1, j);
+    }
+}
+template <typename T, class ST>
+__device__ __forceinline__ void st_pair(const ST& st, int o, int col, int k, T a, T b) {
+    if constexpr (pair_io<ST>::value) {
+        st.st2(o, col, k, a, b);
+    } else {
+        st(o, col, k, a);
+        st(o, col + 1, k, b);
+    }
+}
+
+// Plane-bound functors.  A tile pass works on one plane o, so a functor that picks
+// its source or destination by o (which field, which level, which derivative) can
+// do that once per tile instead of once per element.  plane_ld(f) / plane_st(f)
+// wrap a callable f(o) that returns the accessor of plane o:
+//   loads:  g(col, pt) -> T2        the values of columns col and col + 1 (col even)
+//   stores: g(col, pt, a, b, m)     a to column col if m & 1, b to col + 1 if m & 2
+// Every pass binds its functors once per tile (bind_ld / bind_st); a functor of
+// the per-element form (ld(o, col, pt), st(o, col, pt, v)) binds to itself.
+template <class F>
+struct PlaneLd {
+    F f;
+};
+template <class F>
+struct PlaneSt {
+    F f;
+};
+template <class F>
+inline PlaneLd<F> plane_ld(F f) {
+    return PlaneLd<F>{f};
+}
+template <class F>
+inline PlaneSt<F> plane_st(F f) {
+    return PlaneSt<F>{f};
+}
+template <class G>
+struct BoundLd {
+    G g;
+};
+template <class G>
+struct BoundSt {
+    G g;
+};
+template <class LD>
+__device__ __forceinline__ const LD& bind_ld(const LD& f, int) {
+    return f;
+}
+template <class ST>
+__device__ __forceinline__ const ST& bind_st(const ST& f, int) {
+    return f;
+}
+template <class F>
+__device__ __forceinline__ auto bind_ld(const PlaneLd<F>& f, int o) {
+    return BoundLd<decltype(f.f(o))>{f.f(o)};
+}
+template <class F>
+__device__ __forceinline__ auto bind_st(const PlaneSt<F>& f, int o) {
+    return BoundSt<decltype(f.f(o))>{f.f(o)};
+}
+template <typename T, class G>
+__device__ __forceinline__ void ld_pair(const BoundLd<G>& b, int, int col, int j, T& x, T& y) {
+    const auto v = b.g(col, j);
+    x = (T)v.x;
+    y = (T)v.y;
+}
+template <typename T, class G>
+__device__ __forceinline__ void st_pair(const BoundSt<G>& b, int, int col, int k, T x, T y) {
+    b.g(col, k, x, y, 3);
+}
+// Single elements (the generic pass): a bound load reads the pair and keeps one
+// value; a bound store writes one column of the pair.
+template <typename T, class LD>
+__device__ __forceinline__ T ld_one(const LD& ld, int o, int col, int j) {
+    return (T)ld(o, col, j);
+}
+template <typename T, class G>
+__device__ __forceinline__ T ld_one(const BoundLd<G>& b, int, int col, int j) {
+    const auto v = b.g(col & ~1, j);
+    return (col & 1) ? (T)v.y : (T)v.x;
+}
+template <typename T, class ST>
+__device__ __forceinline__ void st_one(const ST& st, int o, int col, int k, T v) {
+    st(o, col, k, v);
+}
+template <typename T, class G>
+__device__ __forceinline__ void st_one(const BoundSt<G>& b, int, int col, int k, T v) {
+    if (col & 1) b.g(col - 1, k, v, v, 2);
+    else b.g(col, k, v, v, 1);
+}
+// Accessor helpers for plane-bound functors: the pair (p[0], p[1]) of an even
+// index as one vector access, and a masked pair store.
+template <typename T>
+__device__ __forceinline__ typename C2<T>::t ldv2(const T* p) {
+    return *reinterpret_cast<const typename C2<T>::t*>(p);
+}
+template <typename T>
+__device__ __forceinline__ typename C2<T>::t ldv2_ro(const T* p) {
+    return __ldg(reinterpret_cast<const typename C2<T>::t*>(p));
+}
+template <typename T>
+__device__ __forceinline__ typename C2<T>::t mk2(T a, T b) {
+    typename C2<T>::t v;
+    v.x = a;
+    v.y = b;
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ void stv2m(T* p, int m, T a, T b) {
+    if (m == 3) *reinterpret_cast<typename C2<T>::t*>(p) = mk2(a, b);
+    else if (m == 1) p[0] = a;
+    else p[1] = b;
+}
+
 template <typename T>
 inline size_t fft_pass_smem(int n, int tc) {
     return sizeof(typename C2<T>::t) * ((size_t)n + (size_t)tc * padded_len(n));
@@ -314,6 +445,8 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
     const int o = blockIdx.y;
     const int c0 = blockIdx.x * tc;
     const int nthr = NS ? FFT_THREADS : (int)blockDim.x;
+    const auto& ldb = bind_ld(ld, o);
+    const auto& stb = bind_st(st, o);
     const int total = tc * n;
 
     for (int i = threadIdx.x; i < n; i += nthr) tw[i] = twg[i];
@@ -328,7 +461,7 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
             else if (NS) { j = idx % n; c = idx / n; }
             else         { j = (int)((uint32_t)idx - fdiv((uint32_t)idx, dn) * (uint32_t)n); c = (int)fdiv((uint32_t)idx, dn); }
             const int col = c0 + c;
-            vals[u] = (idx < total && col < ncols) ? (T)ld(o, col, j) : T(0);
+            vals[u] = (idx < total && col < ncols) ? ld_one<T>(ldb, o, col, j) : T(0);
         }
 #pragma unroll
         for (int u = 0; u < FFT_UNROLL; u++) {
@@ -381,7 +514,7 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
             const T2 a = z[pad16(k)];
             val = (c & 1) ? a.y : a.x;
         }
-        st(o, col, k, val * sc);
+        st_one<T>(stb, o, col, k, val * sc);
     }
 }
 
@@ -397,38 +530,10 @@ k_fft_pass(FftPlan plan, const typename C2<T>::t* __restrict__ twg, int ncols, i
 // arithmetic folds into immediate offsets.
 // ---------------------------------------------------------------------------
 
-// Functors that tag `static constexpr bool pair_io = true` provide
-// ld2(o, col, pt) -> T2 and st2(o, col, pt, a, b) for the adjacent columns
-// (col, col+1), col even; others get two scalar calls.
-template <class F, class = void>
-struct pair_io : std::false_type {};
-template <class F>
-struct pair_io<F, std::void_t<decltype(F::pair_io)>> : std::integral_constant<bool, F::pair_io> {};
-
-template <typename T, class LD>
-__device__ __forceinline__ void ld_pair(const LD& ld, int o, int col, int j, T& a, T& b) {
-    if constexpr (pair_io<LD>::value) {
-        const auto v = ld.ld2(o, col, j);
-        a = v.x;
-        b = v.y;
-    } else {
-        a = (T)ld(o, col, j);
-        b = (T)ld(o, col + 1, j);
-    }
-}
-template <typename T, class ST>
-__device__ __forceinline__ void st_pair(const ST& st, int o, int col, int k, T a, T b) {
-    if constexpr (pair_io<ST>::value) {
-        st.st2(o, col, k, a, b);
-    } else {
-        st(o, col, k, a);
-        st(o, col + 1, k, b);
-    }
-}
 
 template <typename T, int NS, int LTCS, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST>
 __global__ void __launch_bounds__(FFT_THREADS, 3)
-k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
+k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld_, ST st_) {
     using T2 = typename C2<T>::t;
     static_assert(NS == 128 || NS == 256, "static lengths: 128, 256");
     static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
@@ -443,6 +548,8 @@ k_fft_pass_s(const typename C2<T>::t* __restrict__ twg, T sc, LD ld, ST st) {
     const int tid = threadIdx.x;
     const int o = blockIdx.y;
     const int c0 = blockIdx.x * TC;
+    const auto& ld = bind_ld(ld_, o);
+    const auto& st = bind_st(st_, o);
     for (int i = tid; i < N; i += TH) tw[i] = twg[i];
 
     if constexpr (INV) {
@@ -654,13 +761,15 @@ __device__ __forceinline__ T2 shfl_xor_c(T2 v, int m) {
 // (classes j and 16 - j) instead of going through shared memory again.
 template <typename T, int NPT, bool INV, bool LOAD_CF, bool STORE_CF, class LD, class ST, class HK>
 __device__ __forceinline__ void fft_r_tile(const typename C2<T>::t* __restrict__ tw, typename C2<T>::t* buf, T sc,
-                                           const LD& ld, const ST& st, int o, int c0, const HK& hk) {
+                                           const LD& ld_, const ST& st_, int o, int c0, const HK& hk) {
     using T2 = typename C2<T>::t;
     static_assert(!INV || LOAD_CF, "reverse passes load column-contiguous tiles");
     static_assert(INV || STORE_CF, "forward passes store column-contiguous tiles");
     constexpr int N = FFT_R_N, H = N / 2, NP = NPT, PL = FFT_R_PL;
     static_assert(NP == 8 || NP == 16, "partner classes must share a warp");
     const int tid = threadIdx.x;
+    const auto& ld = bind_ld(ld_, o);
+    const auto& st = bind_st(st_, o);
     // pair-major (pair index on the lanes: column-contiguous global access) with the
     // partner class order, and point-major (point index on the lanes: point-contiguous
     // global access)

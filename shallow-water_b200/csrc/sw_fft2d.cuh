@@ -31,6 +31,15 @@ struct StOff {
     template <class V>
     __device__ __forceinline__ void operator()(int o, int c, int p, V v) const { f(o0 + o, c, p, v); }
 };
+// plane-bound functors of a chunk: bind to plane o0 + o
+template <class F>
+__device__ __forceinline__ auto bind_ld(const LdOff<PlaneLd<F>>& f, int o) {
+    return bind_ld(f.f, f.o0 + o);
+}
+template <class F>
+__device__ __forceinline__ auto bind_st(const StOff<PlaneSt<F>>& f, int o) {
+    return bind_st(f.f, f.o0 + o);
+}
 // intermediate addressed [pt + ng*col] (point index contiguous)
 template <typename T>
 struct MidPC {
@@ -478,6 +487,43 @@ template <typename T>
 __device__ __forceinline__ T dmul_t(int a, int ng, T v) {
     return (T)imul(a, ng) * v;
 }
+// Plane-bound access to one spectral plane s ([kx + ng*ky], Hermitian-packed) at
+// the kx pair (kx, kx + 1), kx even: kind 0 the values, 1 d/dx, 2 d/dy, with the
+// products of dmul_t (so equal to the per-element functors' results).
+template <typename T>
+__device__ __forceinline__ typename C2<T>::t spec_pair(const T* s, int kind, int kx, int ky, int ng) {
+    if (kind == 0) return ldv2(s + kx + ng * ky);
+    if (kind == 1)
+        return mk2(dmul_t(kx, ng, s[mirror(kx, ng) + ng * ky]), dmul_t(kx + 1, ng, s[mirror(kx + 1, ng) + ng * ky]));
+    const auto v = ldv2(s + kx + ng * mirror(ky, ng));
+    return mk2(dmul_t(ky, ng, v.x), dmul_t(ky, ng, v.y));
+}
+// Accessors of one plane ([col + ng*pt]) for plane-bound functors: plain values,
+// plain stores, and stores of the product with a float64 operator table (the
+// dealiasing filter, glap) rounded to T, as (T)(op[i] * (double)v).
+template <typename T>
+struct PairLd {
+    const T* s;
+    int ng;
+    __device__ __forceinline__ typename C2<T>::t operator()(int c, int p) const { return ldv2(s + c + ng * p); }
+};
+template <typename T>
+struct PairSt {
+    T* d;
+    int ng;
+    __device__ __forceinline__ void operator()(int c, int p, T a, T b, int m) const { stv2m(d + c + ng * p, m, a, b); }
+};
+template <typename T>
+struct PairStOp {
+    T* d;
+    const double* op;
+    int ng;
+    __device__ __forceinline__ void operator()(int c, int p, T a, T b, int m) const {
+        const int i = c + ng * p;
+        const double2 f = ldv2_ro(op + i);
+        stv2m(d + i, m, (T)(f.x * (double)a), (T)(f.y * (double)b));
+    }
+};
 // Parseval weight of one axis for the Hermitian packing: 1 at 0 and ng/2, else 2.
 __device__ __forceinline__ double pweight(int a, int ng) { return (a == 0 || 2 * a == ng) ? 1.0 : 2.0; }
 

@@ -930,16 +930,14 @@ struct Solver {
             SV[p] = (T)(dmul(ky, ng) * (rlap[my] * dsq[my]) + dmul(kx, ng) * (rlap[mx] * wkb(mx)));
         });
         fft.spctop(st, 4 * ML,
-            [=] __device__(int o, int kx, int ky) -> T {
+            plane_ld([=] __device__(int o) {
                 const int which = o & 3, q = o >> 2;
-                const T* g = which == 0 ? SR : which == 1 ? SZ : which == 2 ? SU : SV;
-                return g[(size_t)q * n2 + kx + ng * ky];
-            },
-            [=] __device__(int o, int iy, int ix, T val) {
+                return PairLd<T>{(which == 0 ? SR : which == 1 ? SZ : which == 2 ? SU : SV) + (size_t)q * n2, ng};
+            }),
+            plane_st([=] __device__(int o) {
                 const int which = o & 3, q = o >> 2;
-                T* out = which == 0 ? R : which == 1 ? ZE : which == 2 ? U : V;
-                out[(size_t)q * n2 + iy + ng * ix] = val;
-            });
+                return PairSt<T>{(which == 0 ? R : which == 1 ? ZE : which == 2 ? U : V) + (size_t)q * n2, ng};
+            }));
         // mean flow (uio, vio): per-plane sums of u*r and v*r
         double* sums = red_out.p;
         reduce_groups<2>(st, ML, n2, 0u,
@@ -1532,97 +1530,154 @@ struct Solver {
         const int o_z = 3 * ML, o_p = o_z + (mixed ? 0 : Mnz);
         const int o_u = o_p + (ps_ready ? 0 : ML), o_v = o_u + (uv_ready ? 0 : ML), o_h = o_v + (uv_ready ? 0 : ML);
         const int n1 = o_h + (mixed ? 0 : M);
+        // (plane-bound functors: the field, level and product of a plane are chosen
+        // once per tile; pairs of columns move as one vector access)
         fft.ptospc(st, n1,
-            [=] __device__(int o, int iy, int ix) -> T {
-                const int pi = iy + ng * ix;
+            plane_ld([=] __device__(int o) {
+                int kind = 0;  // 0 plain, 1 1/(1+r), 2 (u or v) r
+                const T *s = nullptr, *rr = nullptr;
                 if (o < o_z) {
                     const int q = o / 3, which = o - 3 * q;
-                    const size_t p = (size_t)q * n2 + pi;
-                    return which == 0 ? T(1) / (R[p] + T(1)) : (which == 1 ? U[p] : V[p]) * R[p];
-                }
-                if (o < o_p) {
+                    rr = R + (size_t)q * n2;
+                    s = (which == 1 ? U : V) + (size_t)q * n2;
+                    kind = which == 0 ? 1 : 2;
+                } else if (o < o_p) {
                     const int k = o - o_z, m = k / nz, iz = 1 + k % nz;
-                    return Z[(size_t)(m * L + iz) * n2 + pi];
+                    s = Z + (size_t)(m * L + iz) * n2;
+                } else if (o < o_u) {
+                    s = PN + (size_t)(o - o_p) * n2;
+                } else if (o < o_v) {
+                    s = U + (size_t)(o - o_u) * n2;
+                } else if (o < o_h) {
+                    s = V + (size_t)(o - o_v) * n2;
+                } else {
+                    s = Z + (size_t)((o - o_h) * L + nz) * n2;
                 }
-                if (o < o_u) return PN[(size_t)(o - o_p) * n2 + pi];
-                if (o < o_v) return U[(size_t)(o - o_u) * n2 + pi];
-                if (o < o_h) return V[(size_t)(o - o_v) * n2 + pi];
-                return Z[(size_t)((o - o_h) * L + nz) * n2 + pi];
-            },
-            [=] __device__(int o, int kx, int ky, T val) {
-                const int i = kx + ng * ky;
+                return [=](int iy, int ix) {
+                    const int pi = iy + ng * ix;
+                    if (kind == 0) return ldv2(s + pi);
+                    const auto r2 = ldv2(rr + pi);
+                    if (kind == 1) return mk2(T(1) / (r2.x + T(1)), T(1) / (r2.y + T(1)));
+                    const auto v2 = ldv2(s + pi);
+                    return mk2(v2.x * r2.x, v2.y * r2.y);
+                };
+            }),
+            plane_st([=] __device__(int o) {
+                int kind = 0;  // 0 plain, 1 times a float64 operator, 2 float64 destination
+                T* d = nullptr;
+                double* dd = nullptr;
+                const double* opd = filt;
                 if (o < o_z) {
                     const int q = o / 3, which = o - 3 * q;
-                    const size_t p = (size_t)q * n2 + i;
-                    if (which == 0) Sr[p] = (T)(filt[i] * (double)val);
-                    else (which == 1 ? SA : SB)[p] = val;
-                    return;
-                }
-                if (o < o_p) {
+                    d = (which == 0 ? Sr : which == 1 ? SA : SB) + (size_t)q * n2;
+                    kind = which == 0 ? 1 : 0;
+                } else if (o < o_p) {
                     const int k = o - o_z, m = k / nz, iz = 1 + k % nz;
-                    S1[(size_t)(m * L + iz) * n2 + i] = val;
-                    return;
+                    d = S1 + (size_t)(m * L + iz) * n2;
+                } else if (o < o_u) {  // first-guess ps, all levels (see psolve_prepare)
+                    dd = PS + (size_t)(o - o_p) * n2;
+                    kind = 2;
+                } else if (o < o_v) {
+                    d = Su + (size_t)(o - o_u) * n2;
+                } else if (o < o_h) {
+                    d = Sv + (size_t)(o - o_v) * n2;
+                } else {
+                    d = hs + (size_t)(o - o_h) * n2;
+                    opd = glap;
+                    kind = 1;
                 }
-                if (o < o_u) {  // first-guess ps, all levels (see psolve_prepare)
-                    PS[(size_t)(o - o_p) * n2 + i] = (double)val;
-                    return;
-                }
-                if (o < o_v) { Su[(size_t)(o - o_u) * n2 + i] = val; return; }
-                if (o < o_h) { Sv[(size_t)(o - o_v) * n2 + i] = val; return; }
-                hs[(size_t)(o - o_h) * n2 + i] = (T)((double)val * glap[i]);
-            });
+                return [=](int kx, int ky, T a, T b, int mk) {
+                    const int i = kx + ng * ky;
+                    if (kind == 2) {
+                        stv2m(dd + i, mk, (double)a, (double)b);
+                        return;
+                    }
+                    if (kind == 1) {
+                        const double2 f = ldv2_ro(opd + i);
+                        a = (T)(f.x * (double)a);
+                        b = (T)(f.y * (double)b);
+                    }
+                    stv2m(d + i, mk, a, b);
+                };
+            }));
         // P2: inverse transforms: ri, z_x, z_y, rsrc (with A), u/v derivatives, hsrc or HZ
         const int q_x = ML, q_r = ML + 2 * Mnz, q_d = q_r + ML, q_h = q_d + 4 * ML;
         const int n2t = q_h + (mixed ? ML : M);
         fft.spctop(st, n2t,
-            [=] __device__(int o, int kx, int ky) -> T {
-                const int i = kx + ng * ky;
-                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
-                if (o < q_x) return Sr[(size_t)o * n2 + i];
-                if (o < q_r) {  // z_x, z_y of one level adjacent
-                    const int k = o - q_x, which = k & 1, kk = k >> 1, m = kk / nz, iz = 1 + kk % nz;
-                    const T* sz = S1 + (size_t)(m * L + iz) * n2;
-                    return which == 0 ? dmul_t(kx, ng, sz[mx]) : dmul_t(ky, ng, sz[my]);
-                }
-                if (o < q_d) {
-                    const int q = o - q_r;
-                    const size_t b = (size_t)q * n2;
-                    const double wkb = dmul(kx, ng) * (double)SA[b + mx];
-                    const double wkc = dmul(ky, ng) * (double)SB[b + my];
-                    const T a = (T)(filt[i] * (wkb + wkc));
-                    AA[b + i] = a;
-                    return (T)((double)a + DS[b + i]);
-                }
-                if (o < q_h) {  // u_x, u_y, v_x, v_y of one level adjacent
+            plane_ld([=] __device__(int o) {
+                int kind = 0;  // 0/1/2 value, d/dx, d/dy of s; 3 rsrc (plane b); 4 HZ (plane b)
+                const T* s = nullptr;
+                size_t b = 0;
+                if (o < q_x) {
+                    s = Sr + (size_t)o * n2;
+                } else if (o < q_r) {  // z_x, z_y of one level adjacent
+                    const int k = o - q_x, kk = k >> 1, m = kk / nz, iz = 1 + kk % nz;
+                    s = S1 + (size_t)(m * L + iz) * n2;
+                    kind = 1 + (k & 1);
+                } else if (o < q_d) {
+                    b = (size_t)(o - q_r) * n2;
+                    kind = 3;
+                } else if (o < q_h) {  // u_x, u_y, v_x, v_y of one level adjacent
                     const int k = o - q_d, which = k & 3, q = k >> 2;
-                    const T* sv = (which < 2 ? Su : Sv) + (size_t)q * n2;
-                    return (which & 1) == 0 ? dmul_t(kx, ng, sv[mx]) : dmul_t(ky, ng, sv[my]);
+                    s = (which < 2 ? Su : Sv) + (size_t)q * n2;
+                    kind = 1 + (which & 1);
+                } else if (!mixed) {
+                    s = hs + (size_t)(o - q_h) * n2;
+                } else {
+                    b = (size_t)(o - q_h);
+                    kind = 4;
                 }
-                if (!mixed) return hs[(size_t)(o - q_h) * n2 + i];
-                const int q = o - q_h, m = q / L;
-                const size_t p = (size_t)q * n2 + i;
-                const double wv = hspec[(size_t)M * n2 + (size_t)m * n2 + i];
-                const double zeta_s = QS[p] + COF * (COFI * (COFI * GS[p] - QS[p]) - wv);
-                return (T)(glap[i] * hspec[(size_t)m * n2 + i] + COF * zeta_s);
-            },
-            [=] __device__(int o, int iy, int ix, T val) {
-                const int pi = iy + ng * ix;
-                if (o < q_x) { RI[(size_t)o * n2 + pi] = val; return; }
-                if (o < q_r) {
+                return [=](int kx, int ky) {
+                    if (kind <= 2) return spec_pair(s, kind, kx, ky, ng);
+                    const int i = kx + ng * ky;
+                    if (kind == 3) {
+                        const int myo = ng * mirror(ky, ng);
+                        const double dy = dmul(ky, ng);
+                        const double2 fl = ldv2_ro(filt + i);
+                        const auto sb = ldv2(SB + b + kx + myo);
+                        const double2 dsv = ldv2(DS + b + i);
+                        const double wkb0 = dmul(kx, ng) * (double)SA[b + mirror(kx, ng) + ng * ky];
+                        const double wkb1 = dmul(kx + 1, ng) * (double)SA[b + mirror(kx + 1, ng) + ng * ky];
+                        const T a0 = (T)(fl.x * (wkb0 + dy * (double)sb.x));
+                        const T a1 = (T)(fl.y * (wkb1 + dy * (double)sb.y));
+                        stv2m(AA + b + i, 3, a0, a1);
+                        return mk2((T)((double)a0 + dsv.x), (T)((double)a1 + dsv.y));
+                    }
+                    const int q = (int)b, m = q / L;
+                    auto hz = [&](int j) {
+                        const size_t p = (size_t)q * n2 + j;
+                        const double wv = hspec[(size_t)M * n2 + (size_t)m * n2 + j];
+                        const double zeta_s = QS[p] + COF * (COFI * (COFI * GS[p] - QS[p]) - wv);
+                        return (T)(glap[j] * hspec[(size_t)m * n2 + j] + COF * zeta_s);
+                    };
+                    return mk2(hz(i), hz(i + 1));
+                };
+            }),
+            plane_st([=] __device__(int o) {
+                T* d;
+                bool neg = false;
+                if (o < q_x) {
+                    d = RI + (size_t)o * n2;
+                } else if (o < q_r) {
                     const int k = o - q_x, which = k & 1, kk = k >> 1, m = kk / nz, iz = 1 + kk % nz;
-                    (which == 0 ? ZX : ZY)[(size_t)(m * L + iz) * n2 + pi] = val;
-                    return;
-                }
-                if (o < q_d) { RS[(size_t)(o - q_r) * n2 + pi] = -val; return; }
-                if (o < q_h) {
+                    d = (which == 0 ? ZX : ZY) + (size_t)(m * L + iz) * n2;
+                } else if (o < q_d) {
+                    d = RS + (size_t)(o - q_r) * n2;
+                    neg = true;
+                } else if (o < q_h) {
                     const int k = o - q_d, which = k & 3, q = k >> 2;
-                    T* out = which == 0 ? UX : which == 1 ? UY : which == 2 ? VX : VY;
-                    out[(size_t)q * n2 + pi] = val;
-                    return;
+                    d = (which == 0 ? UX : which == 1 ? UY : which == 2 ? VX : VY) + (size_t)q * n2;
+                } else {
+                    d = (mixed ? HZ : hsrc) + (size_t)(o - q_h) * n2;
                 }
-                if (!mixed) hsrc[(size_t)(o - q_h) * n2 + pi] = val;
-                else HZ[(size_t)(o - q_h) * n2 + pi] = val;
-            });
+                return [=](int iy, int ix, T a, T b, int mk) {
+                    if (neg) {
+                        a = -a;
+                        b = -b;
+                    }
+                    stv2m(d + iy + ng * ix, mk, a, b);
+                };
+            }));
         // P3: w by trapezoidal integration of rsrc
         for_cols(st, M * n2, [=] __device__(int c) {
             const int m = c / n2, i = c - m * n2;
@@ -1638,66 +1693,114 @@ struct Solver {
         });
         // P4: w, the w correction u z_x + v z_y (dealiased), ri z_x, ri z_y
         fft.ptospc(st, 2 * Mnz + 2 * ML,
-            [=] __device__(int o, int iy, int ix) -> T {
-                const int pi = iy + ng * ix;
+            plane_ld([=] __device__(int o) {
+                int kind = 0;  // 0 w, 1 u z_x + v z_y, 2 ri z_x or ri z_y
+                size_t p0;
+                const T* zz = ZX;
                 if (o < 2 * Mnz) {
                     const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
-                    const size_t p = (size_t)(m * L + iz) * n2 + pi;
-                    return which == 0 ? WW[p] : U[p] * ZX[p] + V[p] * ZY[p];
+                    p0 = (size_t)(m * L + iz) * n2;
+                    kind = which;
+                } else {
+                    const int k = o - 2 * Mnz, which = k & 1, q = k >> 1;  // ri z_x, ri z_y of one level adjacent
+                    p0 = (size_t)q * n2;
+                    zz = which == 0 ? ZX : ZY;
+                    kind = 2;
                 }
-                const int k = o - 2 * Mnz, which = k & 1, q = k >> 1;  // ri z_x, ri z_y of one level adjacent
-                const size_t p = (size_t)q * n2 + pi;
-                return RI[p] * (which == 0 ? ZX[p] : ZY[p]);
-            },
-            [=] __device__(int o, int kx, int ky, T val) {
-                const int i = kx + ng * ky;
+                return [=](int iy, int ix) {
+                    const size_t p = p0 + iy + ng * ix;
+                    if (kind == 0) return ldv2(WW + p);
+                    if (kind == 2) {
+                        const auto r2 = ldv2(RI + p), z2 = ldv2(zz + p);
+                        return mk2(r2.x * z2.x, r2.y * z2.y);
+                    }
+                    const auto u2 = ldv2(U + p), zx2 = ldv2(ZX + p), v2 = ldv2(V + p), zy2 = ldv2(ZY + p);
+                    return mk2(u2.x * zx2.x + v2.x * zy2.x, u2.y * zx2.y + v2.y * zy2.y);
+                };
+            }),
+            plane_st([=] __device__(int o) {
+                T* d;
+                bool filtered = true;
                 if (o < 2 * Mnz) {
                     const int which = o / Mnz, k = o - which * Mnz, m = k / nz, iz = 1 + k % nz;
-                    const size_t p = (size_t)(m * L + iz) * n2 + i;
-                    if (which == 0) Sw[p] = val;
-                    else Sd[p] = (T)(filt[i] * (double)val);
-                    return;
+                    d = (which == 0 ? Sw : Sd) + (size_t)(m * L + iz) * n2;
+                    filtered = which != 0;
+                } else {
+                    const int k = o - 2 * Mnz, which = k & 1, q = k >> 1;
+                    d = (which == 0 ? Sx : Sy) + (size_t)q * n2;
                 }
-                const int k = o - 2 * Mnz, which = k & 1, q = k >> 1;
-                (which == 0 ? Sx : Sy)[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
-            });
+                return [=](int kx, int ky, T a, T b, int mk) {
+                    const int i = kx + ng * ky;
+                    if (filtered) {
+                        const double2 f = ldv2_ro(filt + i);
+                        a = (T)(f.x * (double)a);
+                        b = (T)(f.y * (double)b);
+                    }
+                    stv2m(d + i, mk, a, b);
+                };
+            }));
         // P5: w correction, w_x, w_y, sigx, sigy, div(sig)
         fft.spctop(st, 4 * Mnz + 2 * ML,
-            [=] __device__(int o, int kx, int ky) -> T {
-                const int i = kx + ng * ky;
-                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+            plane_ld([=] __device__(int o) {
+                int kind = 0;  // 0 plain s, 1/2 d/dx, d/dy of w + correction, 3 div(sig)
+                const T* s = nullptr;
+                size_t b = 0;
                 if (o < 3 * Mnz) {  // correction, w_x, w_y of one level adjacent
                     const int k = o / 3, which = o - 3 * k, m = k / nz, iz = 1 + k % nz;
-                    const size_t b = (size_t)(m * L + iz) * n2;
-                    if (which == 0) return Sd[b + i];
-                    if (which == 1) return (T)(dmul(kx, ng) * ((double)Sw[b + mx] + (double)Sd[b + mx]));
-                    return (T)(dmul(ky, ng) * ((double)Sw[b + my] + (double)Sd[b + my]));
-                }
-                if (o < 3 * Mnz + 2 * ML) {
+                    b = (size_t)(m * L + iz) * n2;
+                    s = Sd + b;
+                    kind = which;
+                } else if (o < 3 * Mnz + 2 * ML) {
                     const int k = o - 3 * Mnz, which = k / ML, q = k - which * ML;
-                    return (which == 0 ? Sx : Sy)[(size_t)q * n2 + i];
+                    s = (which == 0 ? Sx : Sy) + (size_t)q * n2;
+                } else {
+                    const int k = o - 3 * Mnz - 2 * ML, m = k / nz, iz = 1 + k % nz;
+                    b = (size_t)(m * L + iz) * n2;
+                    kind = 3;
                 }
-                const int k = o - 3 * Mnz - 2 * ML, m = k / nz, iz = 1 + k % nz;
-                const size_t b = (size_t)(m * L + iz) * n2;
-                return (T)(dmul(ky, ng) * (double)Sy[b + my] + dmul(kx, ng) * (double)Sx[b + mx]);
-            },
-            [=] __device__(int o, int iy, int ix, T val) {
-                const int pi = iy + ng * ix;
+                return [=](int kx, int ky) {
+                    if (kind == 0) return ldv2(s + kx + ng * ky);
+                    if (kind == 1) {
+                        const int j0 = mirror(kx, ng) + ng * ky, j1 = mirror(kx + 1, ng) + ng * ky;
+                        return mk2((T)(dmul(kx, ng) * ((double)Sw[b + j0] + (double)Sd[b + j0])),
+                                   (T)(dmul(kx + 1, ng) * ((double)Sw[b + j1] + (double)Sd[b + j1])));
+                    }
+                    const size_t my = b + kx + ng * mirror(ky, ng);
+                    const double dy = dmul(ky, ng);
+                    if (kind == 2) {
+                        const auto w2 = ldv2(Sw + my), d2 = ldv2(Sd + my);
+                        return mk2((T)(dy * ((double)w2.x + (double)d2.x)), (T)(dy * ((double)w2.y + (double)d2.y)));
+                    }
+                    const auto y2 = ldv2(Sy + my);
+                    const double x0 = (double)Sx[b + mirror(kx, ng) + ng * ky];
+                    const double x1 = (double)Sx[b + mirror(kx + 1, ng) + ng * ky];
+                    return mk2((T)(dy * (double)y2.x + dmul(kx, ng) * x0), (T)(dy * (double)y2.y + dmul(kx + 1, ng) * x1));
+                };
+            }),
+            plane_st([=] __device__(int o) {
+                T* d;
+                bool add = false;
                 if (o < 3 * Mnz) {
                     const int k = o / 3, which = o - 3 * k, m = k / nz, iz = 1 + k % nz;
-                    const size_t p = (size_t)(m * L + iz) * n2 + pi;
-                    if (which == 0) WW[p] = WW[p] + val;
-                    else (which == 1 ? WX : WY)[p] = val;
-                    return;
-                }
-                if (o < 3 * Mnz + 2 * ML) {
+                    d = (which == 0 ? WW : which == 1 ? WX : WY) + (size_t)(m * L + iz) * n2;
+                    add = which == 0;
+                } else if (o < 3 * Mnz + 2 * ML) {
                     const int k = o - 3 * Mnz, which = k / ML, q = k - which * ML;
-                    (which == 0 ? SIGX : SIGY)[(size_t)q * n2 + pi] = val;
-                    return;
+                    d = (which == 0 ? SIGX : SIGY) + (size_t)q * n2;
+                } else {
+                    const int k = o - 3 * Mnz - 2 * ML, m = k / nz, iz = 1 + k % nz;
+                    d = D + (size_t)(m * L + iz) * n2;
                 }
-                const int k = o - 3 * Mnz - 2 * ML, m = k / nz, iz = 1 + k % nz;
-                D[(size_t)(m * L + iz) * n2 + pi] = val;
-            });
+                return [=](int iy, int ix, T a, T b, int mk) {
+                    T* dp = d + iy + ng * ix;
+                    if (add) {
+                        const auto w2 = ldv2(dp);
+                        a = w2.x + a;
+                        b = w2.y + b;
+                    }
+                    stv2m(dp, mk, a, b);
+                };
+            }));
         // P6: cpt2's argument and cpsource's dealiased products.  The four values of
         // an element share the theta derivatives of u, v, w: one streaming pass forms
         // them into staging planes (W(8), W(9), W(10), W(17): consumed by P2 and P5),
@@ -1747,28 +1850,24 @@ struct Solver {
             st4(G3 + p, g3);
         });
         fft.ptospc(st, 4 * ML,
-            [=] __device__(int o, int iy, int ix) -> T {
+            plane_ld([=] __device__(int o) {
                 const int which = o & 3, q = o >> 2;
-                const T* g = which == 0 ? G0 : which == 1 ? G1 : which == 2 ? G2 : G3;
-                return g[(size_t)q * n2 + iy + ng * ix];
-            },
-            [=] __device__(int o, int kx, int ky, T val) {
-                const int which = o & 3, q = o >> 2, i = kx + ng * ky;
-                T* out = which == 0 ? Sc : which == 1 ? Spp : which == 2 ? Spq : Spr;
-                out[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
-            });
+                return PairLd<T>{(which == 0 ? G0 : which == 1 ? G1 : which == 2 ? G2 : G3) + (size_t)q * n2, ng};
+            }),
+            plane_st([=] __device__(int o) {
+                const int which = o & 3, q = o >> 2;
+                return PairStOp<T>{(which == 0 ? Sc : which == 1 ? Spp : which == 2 ? Spq : Spr) + (size_t)q * n2, filt, ng};
+            }));
         // P7: cpt2 and the products back to physical space
         fft.spctop(st, 4 * ML,
-            [=] __device__(int o, int kx, int ky) -> T {
+            plane_ld([=] __device__(int o) {
                 const int which = o / ML, q = o - which * ML;
-                const T* in = which == 0 ? Sc : which == 1 ? Spp : which == 2 ? Spq : Spr;
-                return in[(size_t)q * n2 + kx + ng * ky];
-            },
-            [=] __device__(int o, int iy, int ix, T val) {
+                return PairLd<T>{(which == 0 ? Sc : which == 1 ? Spp : which == 2 ? Spq : Spr) + (size_t)q * n2, ng};
+            }),
+            plane_st([=] __device__(int o) {
                 const int which = o / ML, q = o - which * ML;
-                T* out = which == 0 ? C2 : which == 1 ? Pp : which == 2 ? Pq : Pr;
-                out[(size_t)q * n2 + iy + ng * ix] = val;
-            });
+                return PairSt<T>{(which == 0 ? C2 : which == 1 ? Pp : which == 2 ? Pq : Pr) + (size_t)q * n2, ng};
+            }));
         // P8: cpt1 = 0.5 d(cpt2)/dtheta + div(sig); sig *= 2 (coeffs.rs:44-100)
         //     (four elements per thread; the theta derivative is tderiv's one-sided /
         //     centred form with qdzi)
@@ -1825,15 +1924,10 @@ struct Solver {
             }
             st4(G + p, g);
         });
-        fft.ptospc(st, ML,
-            [=] __device__(int q, int iy, int ix) -> T { return G[(size_t)q * n2 + iy + ng * ix]; },
-            [=] __device__(int q, int kx, int ky, T val) {
-                const int i = kx + ng * ky;
-                Sq2[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
-            });
-        fft.spctop(st, ML,
-            [=] __device__(int q, int kx, int ky) -> T { return Sq2[(size_t)q * n2 + kx + ng * ky]; },
-            [=] __device__(int q, int iy, int ix, T val) { Gq[(size_t)q * n2 + iy + ng * ix] = val; });
+        fft.ptospc(st, ML, plane_ld([=] __device__(int q) { return PairLd<T>{G + (size_t)q * n2, ng}; }),
+                   plane_st([=] __device__(int q) { return PairStOp<T>{Sq2 + (size_t)q * n2, filt, ng}; }));
+        fft.spctop(st, ML, plane_ld([=] __device__(int q) { return PairLd<T>{Sq2 + (size_t)q * n2, ng}; }),
+                   plane_st([=] __device__(int q) { return PairSt<T>{Gq + (size_t)q * n2, ng}; }));
         for_planes4(st, ML, n2, [=] __device__(int q, int pi) {
             const int m = q / L, iz = q % L;
             const size_t p = (size_t)q * n2 + pi;
@@ -2158,16 +2252,16 @@ struct Solver {
             for (int m0 = 0; m0 < M; m0 += mchunk) {
                 const int mc = std::min(mchunk, M - m0);
                 launch_pass<float, true, true, false>(st, f32.plan, f32.tw.p, f32.tc, f32.sc, n2z * mc, ng,
-                    [=] __device__(int o, int kx, int ky) -> float {  // d, d_y of one level adjacent
+                    plane_ld([=] __device__(int o) {  // d, d_y of one level adjacent
                         const int mm = o / n2z, k = o - mm * n2z, iz = k >> 1, kind = k & 1;
                         const size_t b = (size_t)((m0 + mm) * L + iz) * n2;
-                        if (kind == 0) {
-                            const size_t j = b + kx + ng * ky;
-                            return D1[j] + Cr[j];
-                        }
-                        const size_t j = b + kx + ng * mirror(ky, ng);
-                        return dmul_t(ky, ng, D1[j] + Cr[j]);
-                    },
+                        return [=](int kx, int ky) {
+                            const size_t j = b + kx + ng * (kind == 0 ? ky : mirror(ky, ng));
+                            const float2 a = ldv2(D1 + j), c = ldv2(Cr + j);
+                            if (kind == 0) return mk2(a.x + c.x, a.y + c.y);
+                            return mk2(dmul_t(ky, ng, a.x + c.x), dmul_t(ky, ng, a.y + c.y));
+                        };
+                    }),
                     MidPC<float>{f32.midp, ng});
                 launch_pass<float, true, true, true>(st, f32.plan, f32.tw.p, f32.tc, f32.sc, 3 * nz * mc, ng,
                     SweepMidLoad<float>{f32.midp, ng, nz}, SweepPhysStore<float>{A, B, C, ng, nz, L, m0});
@@ -2374,19 +2468,38 @@ struct Solver {
         // F = deal(ri * dpn) spectral; spectral u, v (unless reused); spectral z(0)
         const int nf1 = (1 + nuv) * ML;
         fft.ptospc(st, nf1 + M,
-            [=] __device__(int o, int iy, int ix) -> T {
-                if (o >= nf1) return Z[(size_t)((o - nf1) * L) * n2 + iy + ng * ix];
-                const int which = o / ML, q = o - which * ML;
-                const size_t p = (size_t)q * n2 + iy + ng * ix;
-                return which == 0 ? RI[p] * DPN[p] : which == 1 ? U[p] : V[p];
-            },
-            [=] __device__(int o, int kx, int ky, T val) {
-                const int i = kx + ng * ky;
-                if (o >= nf1) { zs0[(size_t)(o - nf1) * n2 + i] = val; return; }
-                const int which = o / ML, q = o - which * ML;
-                if (which == 0) F[(size_t)q * n2 + i] = (T)(filt[i] * (double)val);
-                else (which == 1 ? Su : Sv)[(size_t)q * n2 + i] = val;
-            });
+            plane_ld([=] __device__(int o) {
+                const T *s, *s2 = nullptr;  // s2: second factor of ri * dpn
+                if (o >= nf1) {
+                    s = Z + (size_t)((o - nf1) * L) * n2;
+                } else {
+                    const int which = o / ML, q = o - which * ML;
+                    s = (which == 0 ? RI : which == 1 ? U : V) + (size_t)q * n2;
+                    if (which == 0) s2 = DPN + (size_t)q * n2;
+                }
+                return [=](int iy, int ix) {
+                    const int pi = iy + ng * ix;
+                    const auto a2 = ldv2(s + pi);
+                    if (!s2) return a2;
+                    const auto b2 = ldv2(s2 + pi);
+                    return mk2(a2.x * b2.x, a2.y * b2.y);
+                };
+            }),
+            plane_st([=] __device__(int o) {
+                T* d;
+                const double* opd = nullptr;
+                if (o >= nf1) {
+                    d = zs0 + (size_t)(o - nf1) * n2;
+                } else {
+                    const int which = o / ML, q = o - which * ML;
+                    d = (which == 0 ? F : which == 1 ? Su : Sv) + (size_t)q * n2;
+                    if (which == 0) opd = filt;
+                }
+                return [=](int kx, int ky, T a, T b, int mk) {
+                    if (opd) PairStOp<T>{d, opd, ng}(kx, ky, a, b, mk);
+                    else stv2m(d + kx + ng * ky, mk, a, b);
+                };
+            }));
         // q, delta, ff, ffx, ffy, (ux, uy, vx, vy), z(0) derivatives to physical space.
         // When this stage's main_invert has run, q = zeta - f r pointwise (main_invert
         // sets zeta = spctop(qs + f rhat), r = spctop(rhat)), so q is not transformed.
@@ -2396,34 +2509,43 @@ struct Solver {
         const int nk = 5 - q0 + 2 * nuv;  // kinds per level, level-major
         const int nf2 = nk * ML;
         fft.spctop(st, nf2 + 2 * M,
-            [=] __device__(int o, int kx, int ky) -> T {
-                const int mx = mirror(kx, ng) + ng * ky, my = kx + ng * mirror(ky, ng);
+            plane_ld([=] __device__(int o) {
+                int kind;  // 0/1/2 value, d/dx, d/dy of s; 3 float64 plane sd
+                const T* s = nullptr;
+                const double* sd = nullptr;
                 if (o >= nf2) {
                     const int which = (o - nf2) / M, m = (o - nf2) % M;
-                    const T* s = zs0 + (size_t)m * n2;
-                    return which == 0 ? dmul_t(kx, ng, s[mx]) : dmul_t(ky, ng, s[my]);
+                    s = zs0 + (size_t)m * n2;
+                    kind = 1 + which;
+                } else {
+                    const int q = o / nk, which = o - nk * q + q0;
+                    if (which < 2) {
+                        sd = (which == 0 ? QS : DS) + (size_t)q * n2;
+                        kind = 3;
+                    } else {
+                        const int w2 = which - 2;  // 0..2: F, F_x, F_y; 3..6: u_x, u_y, v_x, v_y
+                        s = (w2 < 3 ? F : w2 < 5 ? Su : Sv) + (size_t)q * n2;
+                        kind = w2 < 3 ? w2 : (w2 - 3) % 2 + 1;  // 0 value, 1 d/dx, 2 d/dy
+                    }
                 }
-                const int q = o / nk, which = o - nk * q + q0;
-                if (which < 2) return (T)(which == 0 ? QS : DS)[(size_t)q * n2 + kx + ng * ky];
-                const int w2 = which - 2;  // 0..2: F, F_x, F_y; 3..6: u_x, u_y, v_x, v_y
-                const T* s = (w2 < 3 ? F : w2 < 5 ? Su : Sv) + (size_t)q * n2;
-                const int kind = w2 < 3 ? w2 : (w2 - 3) % 2 + 1;  // 0 value, 1 d/dx, 2 d/dy
-                if (kind == 0) return s[kx + ng * ky];
-                if (kind == 1) return dmul_t(kx, ng, s[mx]);
-                return dmul_t(ky, ng, s[my]);
-            },
-            [=] __device__(int o, int iy, int ix, T val) {
-                const int i = iy + ng * ix;
+                return [=](int kx, int ky) {
+                    if (kind < 3) return spec_pair(s, kind, kx, ky, ng);
+                    const double2 v = ldv2(sd + kx + ng * ky);
+                    return mk2((T)v.x, (T)v.y);
+                };
+            }),
+            plane_st([=] __device__(int o) {
+                T* d;
                 if (o >= nf2) {
                     const int which = (o - nf2) / M, m = (o - nf2) % M;
-                    (which == 0 ? zx0 : zy0)[(size_t)m * n2 + i] = val;
-                    return;
+                    d = (which == 0 ? zx0 : zy0) + (size_t)m * n2;
+                } else {
+                    const int q = o / nk, which = o - nk * q + q0;
+                    d = (which == 0 ? Q : which == 1 ? DD : which == 2 ? FF : which == 3 ? FX : which == 4 ? FY
+                         : which == 5 ? UX : which == 6 ? UY : which == 7 ? VX : VY) + (size_t)q * n2;
                 }
-                const int q = o / nk, which = o - nk * q + q0;
-                T* out = which == 0 ? Q : which == 1 ? DD : which == 2 ? FF : which == 3 ? FX : which == 4 ? FY
-                       : which == 5 ? UX : which == 6 ? UY : which == 7 ? VX : VY;
-                out[(size_t)q * n2 + i] = val;
-            });
+                return PairSt<T>{d, ng};
+            }));
         // products to spectral space: the six products of an element are formed in
         // one streaming pass into staging planes (W(0..4), W(7): the pressure
         // sweep's work planes and F, all consumed by now), then transformed
@@ -2484,16 +2606,16 @@ struct Solver {
             st4(G3 + p, g3);
         });
         fft.ptospc(st, 6 * ML,  // level-major
-            [=] __device__(int o, int iy, int ix) -> T {
+            plane_ld([=] __device__(int o) {
                 const int q = o / 6, which = o - 6 * q;
                 const T* g = which == 0 ? G0 : which == 1 ? G1 : which == 2 ? G2 : which == 3 ? G3 : which == 4 ? G4 : G5;
-                return g[(size_t)q * n2 + iy + ng * ix];
-            },
-            [=] __device__(int o, int kx, int ky, T val) {
+                return PairLd<T>{g + (size_t)q * n2, ng};
+            }),
+            plane_st([=] __device__(int o) {
                 const int q = o / 6, which = o - 6 * q;
                 T* out = which == 0 ? S0 : which == 1 ? S1 : which == 2 ? S2 : which == 3 ? S3 : which == 4 ? S4 : S5;
-                out[(size_t)q * n2 + kx + ng * ky] = val;
-            });
+                return PairSt<T>{out + (size_t)q * n2, ng};
+            }));
         // combine in spectral space
         for_planes(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L;
