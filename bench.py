@@ -334,8 +334,10 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
     if full and args.e2e == "on":
         n3 = sp.n3 * M
         fidx = sw._native.FIELD_INDEX
+        # the state makes a round trip through host memory every step: each step
+        # uploads what the previous step downloaded, so the run follows one trajectory
         pinned = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
-        outs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs")}
+        outs = pinned
         for k in pinned:
             sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(pinned[k].data_ptr(), sw._native._dp), n3))
         e2e_steps = max(2, min(args.steps, 10))
@@ -351,8 +353,9 @@ def run_arm(sw, args, precision, rank, world, local, full=True):
         torch.cuda.synchronize()
         e2e_seq = time.perf_counter() - t0
         res["e2e"] = {"value": replica_throughput(e2e_steps * M, e2e_seq, world, "cuda"), "unit": UNIT,
-                      "h2d_bytes_per_step": 4 * n3 * 8, "d2h_bytes_per_step": 3 * n3 * 8, "steps": e2e_steps,
-                      "mode": "one context, each copy and step waited for"}
+                      "h2d_bytes_per_step": 4 * n3 * 8, "d2h_bytes_per_step": 4 * n3 * 8, "steps": e2e_steps,
+                      "mode": "one context, each copy and step waited for; each step uploads the state "
+                              "the previous step downloaded"}
         if M >= 2 and M % 2 == 0:
             pipe = e2e_pipelined(sw, L, args, M, prec, local, rank, tune, e2e_steps, world, barrier)
             res["e2e_sequential"] = res["e2e"]
@@ -369,9 +372,11 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
     """End-to-end member-steps/s through the C ABI with host buffers: the ensemble
     as two contexts of M/2 members on their own streams.  Every step of every
     member uploads qs, ds, gs, pn from pinned host memory (sw_state_set_all_async),
-    advances (sw_advance_async) and downloads qs, ds, gs (sw_state_get_all_async);
-    one group's copies overlap the other group's step.  Timed on the host clock from
-    the first copy to the sync that completes the last download."""
+    advances (sw_advance_async) and downloads qs, ds, gs, pn (sw_state_get_all_async)
+    into the same buffers, which the next step uploads, so the run follows one
+    trajectory through host memory; one group's copies overlap the other group's
+    step.  Timed on the host clock from the first copy to the sync that completes
+    the last download."""
     import torch
     fidx = sw._native.FIELD_INDEX
     half = M // 2
@@ -390,7 +395,7 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
         sw._native.check(L.sw_advance(sp.ctx, 1, 1))  # captures the step graph
         n3 = sp.n3 * half
         ins = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs", "pn")}
-        outs = {k: torch.empty(n3, dtype=torch.float64, pin_memory=True) for k in ("qs", "ds", "gs")}
+        outs = ins  # stream order: a step's download lands before the next step's upload reads it
         for k, buf in ins.items():
             sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
         groups.append((sp, n3, ins, outs))
@@ -412,7 +417,7 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
     for g in groups:
         g[0].close()
     return {"value": replica_throughput(steps * M, secs, world, "cuda"), "unit": UNIT,
-            "h2d_bytes_per_step": 4 * nall * 8, "d2h_bytes_per_step": 3 * nall * 8, "steps": steps,
+            "h2d_bytes_per_step": 4 * nall * 8, "d2h_bytes_per_step": 4 * nall * 8, "steps": steps,
             "mode": "two contexts of M/2 members on their own streams; one group's copies overlap the other's "
                     "step; one sync at the end"}
 

@@ -698,6 +698,10 @@ struct Solver {
             SW_CUDA(cudaMemset(pnorm.p, 0, sizeof(double) * M));
             sweep_kind.alloc(1);
             SW_CUDA(cudaMemset(sweep_kind.p, 0, sizeof(int)));
+            xh.alloc(3 * nf);
+            SW_CUDA(cudaMemset(xh.p, 0, sizeof(double) * 3 * nf));
+            xflag.alloc(3);
+            SW_CUDA(cudaMemset(xflag.p, 0, 3 * sizeof(int)));
             SW_CUDA(cudaStreamSynchronize(st));
             for (auto& e : step_exec)
                 if (e) {
@@ -708,6 +712,57 @@ struct Solver {
         } else {
             require(false, SW_ERR_ARG, "correction sweeps need the float64 solver");
         }
+    }
+
+    // Mixed path: the first iterate of each pressure solve of a step is predicted
+    // from the previous step, where the reference starts from the previous solve's
+    // solution.  A step solves three times, in slots j = 0 (at the step's start, the
+    // ggen solve), 1 (after the predictor) and 2 (after the corrector).  At the start
+    // of slot j of step n, ps holds the solution of the solve before it (slot j - 1
+    // of step n, or slot 2 of step n - 1), and the first iterate is that plus the
+    // change between the same two slots one step earlier:
+    //   ps <- ps + (H[j] - H[j-1])     H[j] = solution of slot j in step n - 1
+    // then H[j-1] <- the old ps.  The iteration and its fixed point are unchanged;
+    // a nearer first iterate needs fewer sweeps.  A member whose predicted change is
+    // larger than ps itself (|H[j] - H[j-1]| > |ps|: a history from another run), or
+    // whose history is not yet written, keeps ps.  Steps without the ggen solve
+    // clear the history.
+    void extrapolate_guess(int j) {
+        const int n2 = this->n2, L = this->L, ML = this->ML, M = this->M;
+        const int jp = (j + 2) % 3;
+        const long long nm = (long long)L * n2;
+        double* PS = ps;
+        double *Hj = xh.p + (size_t)j * nf, *Hp = xh.p + (size_t)jp * nf;
+        int* fl = xflag.p;
+        double* sums = red_out.p + (size_t)6 * ML;  // 2 M values (red_out holds 8 ML + 64)
+        reduce_groups<2>(st, M, nm, 0u,
+            [=] __device__(int g, long long i) {
+                const size_t p = (size_t)g * nm + i;
+                const double d = Hj[p] - Hp[p];
+                RedVals<2> rv;
+                rv.v[0] = d * d;
+                rv.v[1] = PS[p] * PS[p];
+                return rv;
+            }, red_partial.p, sums);
+        for_planes4(st, ML, n2, [=] __device__(int q, int i) {
+            const int m = q / L;
+            const size_t p = (size_t)q * n2 + i;
+            double c[4];
+            ld4(PS + p, c);
+            if (fl[j] && fl[jp] && sums[2 * m] <= sums[2 * m + 1]) {
+                double a[4], b[4], o[4];
+                ld4(Hj + p, a);
+                ld4(Hp + p, b);
+#pragma unroll
+                for (int e = 0; e < 4; e++) o[e] = c[e] + (a[e] - b[e]);
+                st4(PS + p, o);
+            }
+            st4(Hp + p, c);
+        });
+        for_cols(st, 1, [=] __device__(int) { fl[jp] = 1; });
+    }
+    void reset_guess_history() {
+        if (xflag.p) SW_CUDA(cudaMemsetAsync(xflag.p, 0, 3 * sizeof(int), st));
     }
 
     // Stop rule of the correction sweeps (the mixed path); the captured step graphs
@@ -2092,33 +2147,68 @@ struct Solver {
                     out[e] = (TS)s;
                 }
             } else {
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const size_t pe = p + e, ce = cb + e;
-                    auto P = [&](int l) { return l >= nz ? 0.0 : (double)A[ce + (size_t)l * n2]; };
-                    auto X = [&](int l) { return l >= nz ? 0.0 : (double)B[ce + (size_t)l * n2]; };
-                    auto Y = [&](int l) { return l >= nz ? 0.0 : (double)C[ce + (size_t)l * n2]; };
-                    const double s0 = SP0 ? (double)SP0[pe] : 0.0;
-                    double s;
-                    if (iz == 0) {
-                        const double d2 = (2.0 * P(0) - 5.0 * P(1) + 4.0 * P(2) - P(3)) * dzisq;
-                        s = s0 + (double)C2[pe] * d2;
-                    } else {
-                        // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238)
-                        auto ext = [&](auto F) {
-                            const double a1 = (F(nz) - F(nz - 2)) * hdzi;
-                            const double d1 = (F(nz) - 2.0 * F(nz - 1) + F(nz - 2)) * dzisq;
-                            const double d2 = (F(nz - 1) - 2.0 * F(nz - 2) + F(nz - 3)) * dzisq;
-                            return a1 + dz2 * (3.0 * d1 - d2);
-                        };
-                        const double dxt = ext(X), dyt = ext(Y), dpdt = ext(P);
-                        const double d1 = (P(nz) - 2.0 * P(nz - 1) + P(nz - 2)) * dzisq;
-                        const double d2 = (P(nz - 1) - 2.0 * P(nz - 2) + P(nz - 3)) * dzisq;
-                        const double d2pdt2 = 2.0 * d1 - d2;
-                        s = s0 + (double)SIGX[pe] * dxt + (double)SIGY[pe] * dyt;
-                        s += (double)C2[pe] * d2pdt2 + (double)C1[pe] * dpdt;
+                // boundary levels: the same stencils, four elements per 16-byte load
+                // (levels at or above nz hold p = 0)
+                auto lv4 = [&](const TS* f, int l, double(&v)[4]) {
+                    if (l >= nz) {
+                        v[0] = v[1] = v[2] = v[3] = 0.0;
+                        return;
                     }
-                    out[e] = (TS)s;
+                    TS t[4];
+                    ld4(f + cb + (size_t)l * n2, t);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) v[e] = (double)t[e];
+                };
+                double s0[4] = {0.0, 0.0, 0.0, 0.0};
+                if (SP0) {
+                    TS t[4];
+                    ld4(SP0 + p, t);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) s0[e] = (double)t[e];
+                }
+                TS c2[4];
+                ld4(C2 + p, c2);
+                if (iz == 0) {
+                    double P0[4], P1[4], P2[4], P3[4];
+                    lv4(A, 0, P0);
+                    lv4(A, 1, P1);
+                    lv4(A, 2, P2);
+                    lv4(A, 3, P3);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const double d2 = (2.0 * P0[e] - 5.0 * P1[e] + 4.0 * P2[e] - P3[e]) * dzisq;
+                        out[e] = (TS)(s0[e] + (double)c2[e] * d2);
+                    }
+                } else {
+                    // extrapolation to iz = nz from nz-1, nz-2 (psolve.rs:232-238);
+                    // F[j] holds level nz - j
+                    double Pl[4][4], Xl[4][4], Yl[4][4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        lv4(A, nz - j, Pl[j]);
+                        lv4(B, nz - j, Xl[j]);
+                        lv4(C, nz - j, Yl[j]);
+                    }
+                    TS sx[4], sy[4], c1[4];
+                    ld4(SIGX + p, sx);
+                    ld4(SIGY + p, sy);
+                    ld4(C1 + p, c1);
+                    auto ext = [&](const double(&F)[4][4], int e) {
+                        const double a1 = (F[0][e] - F[2][e]) * hdzi;
+                        const double d1 = (F[0][e] - 2.0 * F[1][e] + F[2][e]) * dzisq;
+                        const double d2 = (F[1][e] - 2.0 * F[2][e] + F[3][e]) * dzisq;
+                        return a1 + dz2 * (3.0 * d1 - d2);
+                    };
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const double dxt = ext(Xl, e), dyt = ext(Yl, e), dpdt = ext(Pl, e);
+                        const double d1 = (Pl[0][e] - 2.0 * Pl[1][e] + Pl[2][e]) * dzisq;
+                        const double d2 = (Pl[1][e] - 2.0 * Pl[2][e] + Pl[3][e]) * dzisq;
+                        const double d2pdt2 = 2.0 * d1 - d2;
+                        double s = s0[e] + (double)sx[e] * dxt + (double)sy[e] * dyt;
+                        s += (double)c2[e] * d2pdt2 + (double)c1[e] * dpdt;
+                        out[e] = (TS)s;
+                    }
                 }
             }
             st4(SRC + p, out);
@@ -2363,6 +2453,7 @@ struct Solver {
     int psolve(int nitmax, int* iters_out, double* errp_out) {
         if (nitmax <= 0) nitmax = 100;
         psolve_prepare(nitmax);
+        if (refine32 && guess_slot >= 0) extrapolate_guess(guess_slot);
         int sweeps = 0;
         int* hctl = reinterpret_cast<int*>(h_pinned);
         while (true) {
@@ -2394,6 +2485,7 @@ struct Solver {
     void psolve_captured(int nitmax, int slot) {
         if (nitmax <= 0) nitmax = 100;
         psolve_prepare(nitmax);
+        if (refine32 && guess_slot >= 0) extrapolate_guess(guess_slot);
         cudaStreamCaptureStatus cs;
         cudaGraph_t g;
         const cudaGraphNode_t* deps = nullptr;
@@ -2894,9 +2986,10 @@ struct Solver {
         double e = 0.0;
         last_sweeps[0] = last_sweeps[1] = last_sweeps[2] = 0;
         StepHints hints(*this);
+        if (!ggen) reset_guess_history();
         if (ggen) {
             main_invert();
-            hints.before_psolve(false);
+            hints.before_psolve(false, 0);
             int stt = psolve(100, &it, &e);
             last_sweeps[0] = it;
             if (stt) return stt;
@@ -2907,7 +3000,7 @@ struct Solver {
         advance_update(true);
         for (int k = 0; k < 2; k++) {
             main_invert();
-            hints.before_psolve(ggen || k > 0);
+            hints.before_psolve(ggen || k > 0, ggen ? 1 + k : -1);
             int stt = psolve(100, &it, &e);
             last_sweeps[1 + k] = it;
             if (stt) return stt;
@@ -2925,16 +3018,23 @@ struct Solver {
     struct StepHints {
         Solver& s;
         explicit StepHints(Solver& sv) : s(sv) {}
-        ~StepHints() { s.hint_uv_spec = s.hint_ps_guess = s.hint_q_phys = false; }
+        ~StepHints() {
+            s.hint_uv_spec = s.hint_ps_guess = s.hint_q_phys = false;
+            s.guess_slot = -1;
+        }
         // main_invert of this stage ran; a psolve of this step already finished?
-        void before_psolve(bool previous_solve_this_step) {
+        // slot: the solve's slot in a ggen step (0, 1, 2) for the mixed path's
+        // predicted first iterate, or -1
+        void before_psolve(bool previous_solve_this_step, int slot = -1) {
             s.hint_uv_spec = s.fused_prepare;
             s.hint_ps_guess = s.fused_prepare && previous_solve_this_step;
             s.hint_q_phys = false;
+            s.guess_slot = slot;
         }
         void before_source(bool invert_this_stage) {
             s.hint_uv_spec = s.hint_ps_guess = false;
             s.hint_q_phys = invert_this_stage;
+            s.guess_slot = -1;
         }
     };
 
@@ -2945,9 +3045,10 @@ struct Solver {
         NvtxRange nv("advance_step_capture");
         SW_CUDA(cudaMemsetAsync(sweeps_dev.p, 0, sizeof(int) * 3 * M, st));
         StepHints hints(*this);
+        if (!ggen) reset_guess_history();
         if (ggen) {
             main_invert();
-            hints.before_psolve(false);
+            hints.before_psolve(false, 0);
             psolve_captured(100, 0);
         }
         diagnose_record();
@@ -2956,7 +3057,7 @@ struct Solver {
         advance_update(true);
         for (int k = 0; k < 2; k++) {
             main_invert();
-            hints.before_psolve(ggen || k > 0);
+            hints.before_psolve(ggen || k > 0, ggen ? 1 + k : -1);
             psolve_captured(100, 1 + k);
             hints.before_source(true);
             source(WD(4), WD(5), WD(7), fused_prepare);
@@ -3058,7 +3159,10 @@ struct Solver {
     // Set by the advance flows around the calls they apply to (see
     // psolve_prepare_fused and source): what earlier work of the same step left.
     bool hint_uv_spec = false;  // Su, Sv hold the spectra of u, v (main_invert ran this stage)
-    bool hint_ps_guess = false; // ps holds the previous solution of this step
+    bool hint_ps_guess = false; // ps holds the previous solution of this step (or, mixed path, of the last step)
+    DevBuf<double> xh;          // mixed path: solutions of the last step's three solves
+    DevBuf<int> xflag;          // which of them are written
+    int guess_slot = -1;        // slot of the next solve in a ggen step (-1: none)
     bool hint_q_phys = false;   // zeta and r are this stage's main_invert output
     bool pending = false;        // steps queued by advance_enqueue and not yet finished
     long long pending_fixed = 0; // their kernel launches outside the sweep loops
