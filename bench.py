@@ -796,9 +796,10 @@ def main():
                        "timing": "K graph-launched steps queued without host round trips, CUDA events on the "
                                  "library's stream",
                        "precision_note": {"fp64": "float64 throughout",
-                                          "mixed": "float64 except the pressure iteration: after a float64 "
-                                                   "reference sweep, float32 correction sweeps on the distance "
-                                                   "from the reference point, stop rule 1e-7",
+                                          "mixed": "float64 fields and most transforms; float32 correction "
+                                                   "sweeps after each solve's float64 reference sweep (stop rule "
+                                                   "1e-7), and float32 transforms for the dealiased products and "
+                                                   "filters of the pressure set-up and of source",
                                           "fp32": "float32 transforms and work fields; not within 1e-5 on "
                                                   "delta/gamma at ng=256"}[args.precision],
                        "fft_autotune": main_arm["tune"]},

@@ -225,9 +225,9 @@ def test_ten_steps_256_all_precisions_vs_oracle(sw, oracle):
     terms, and the gravity-wave part of the step amplifies rounding at high
     wavenumbers, so their relative rounding error is the largest.
     - SW_FP64: every field within 3x the oracle's own float64 spread (SPREAD_256).
-    - SW_MIXED: within the 1e-5 contract on every field (measured ~4e-8 on gamma:
-      float64 everywhere but the pressure sweeps, whose float32 corrections
-      converge to the 1e-7 stop rule).
+    - SW_MIXED: within the 1e-5 contract on every field (measured ~4e-7 on gamma:
+      float32 correction sweeps converging to the 1e-7 stop rule, and float32
+      transforms for the dealiased products of the pressure set-up and source).
     - SW_FP32: its measured accuracy (float32 rounding of physical fields is white
       and the k^2 factors of the gravity-wave terms amplify it: ~1e-4 on delta and
       gamma).  That path does not meet 1e-5 at this size and does not claim it."""

@@ -289,7 +289,8 @@ def test_fp64_ten_steps_vs_oracle(sw, oracle):
 
 
 def test_mixed_ten_steps_vs_oracle(sw, oracle):
-    """SW_MIXED (float32 correction sweeps, stop rule 1e-7) within its 1e-5 rel-L2
+    """SW_MIXED (float32 correction sweeps with stop rule 1e-7, float32 transforms for
+    the dealiased products of the pressure set-up and source) within its 1e-5 rel-L2
     contract on every field, the pressure included."""
     st, ost = _config0(sw, oracle, sw.SW_MIXED, 10)
     for k in ("qs", "ds", "gs", "u", "v", "z", "pn"):
