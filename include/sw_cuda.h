@@ -148,6 +148,18 @@ int sw_set_graphs(sw_ctx* ctx, int enable);
  * value down to 1e-9 is reachable.  SW_ERR_STATE on other precisions.  No reference
  * counterpart. */
 int sw_set_psolve_toler(sw_ctx* ctx, double toler);
+/* Relaxation factor omega in (0, 1] of the pressure iteration: each sweep's new
+ * iterate is x + omega (G(x) - x), where G(x) is the Thomas solve of the source at
+ * x.  The fixed point does not depend on omega; the stop rule measures the
+ * unrelaxed change |G(x) - x|.  The default, 1, is the reference's iteration
+ * (psolve.rs:89-358), whose sweep counts the FP64 path reproduces.  0.8 needs ~40%
+ * fewer sweeps at ng=256, nz=16 (the slowest modes alternate in sign), but the fast
+ * modes then contract by only 1 - omega per sweep, so at the same stop rule the
+ * result lies farther from the fixed point (gamma ~10x farther at ng=256).  With
+ * omega != 1 the float32/float64 sweep schedule of SW_MIXED, which is decided per
+ * context, can make an ensemble member differ from its single run at ~1e-9.
+ * SW_ERR_ARG outside (0, 1].  No reference counterpart. */
+int sw_set_psolve_relax(sw_ctx* ctx, double omega);
 /* Pressure sweeps run on the context so far (each covers all members): out[0] float64
  * sweeps (every sweep of SW_FP64 and SW_FP32, the reference sweeps of SW_MIXED),
  * out[1] float32 correction sweeps of SW_MIXED.  No reference counterpart. */

@@ -9,7 +9,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libswcuda.so")
+# SW_CUDA_LIB_VARIANT=bc loads the bounds-check debug build (libswcuda_bc.so,
+# `python shallow-water_b200/build.py --bounds-check`) instead of the library
+LIB_PATH = os.path.join(HERE, "libswcuda_bc.so" if os.environ.get("SW_CUDA_LIB_VARIANT") == "bc" else "libswcuda.so")
 HEADER = os.path.join(HERE, "..", "include", "sw_cuda.h")
 
 SW_OK, SW_ERR_FACTORISE, SW_ERR_CUDA = 0, 1, 2
@@ -67,6 +69,7 @@ _SIGS = {
     "sw_set_graphs": (_i, [_vp, _i]),
     "sw_set_fft_chunk": (_i, [_vp, _i, _ip]),
     "sw_set_psolve_toler": (_i, [_vp, ctypes.c_double]),
+    "sw_set_psolve_relax": (_i, [_vp, ctypes.c_double]),
     "sw_sweep_counts": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "sw_advance_async": (_i, [_vp, _i, _i]),
     "sw_savegrid": (_i, [_vp, _i, _dp, _dp, _i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
@@ -119,7 +122,7 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise OSError("libswcuda.so not built: run python shallow-water_b200/build.py")
+            raise OSError("%s not built: run python shallow-water_b200/build.py" % os.path.basename(LIB_PATH))
         L = ctypes.CDLL(LIB_PATH)
         for name, (res, args) in _SIGS.items():
             fn = getattr(L, name)

@@ -17,7 +17,22 @@ int fail(int status, const std::string& msg) {
 template <class F>
 int guarded(F&& f) {
     try {
-        return f();
+        const int st = f();
+#ifdef SW_BOUNDS_CHECK
+        // debug build: wait for the call's kernels and report an access outside the
+        // registered allocations (the access itself was skipped)
+        if (st == SW_OK) {
+            unsigned long long addr = 0, bytes = 0;
+            const unsigned long long n = bc::take_fault(&addr, &bytes);
+            if (n) {
+                char msg[200];
+                snprintf(msg, sizeof(msg), "bounds check: %llu device accesses outside the library's allocations or "
+                         "misaligned, the first at 0x%llx (%llu bytes)", n, addr, bytes);
+                return fail(SW_ERR_CUDA, msg);
+            }
+        }
+#endif
+        return st;
     } catch (const Error& e) {
         return fail(e.status, e.what());
     } catch (const std::bad_alloc&) {
@@ -104,6 +119,14 @@ int fft1d_host(int m, int n, double* x, const double* trig, const int factors[5]
 
 namespace sw {
 void record_error(const std::string& msg) { g_last_error = msg; }
+#ifdef SW_BOUNDS_CHECK
+void sw_bc_register(const void* p, size_t bytes, int add) {
+    if (add) bc::add(p, bytes);
+    else bc::remove(p);
+}
+#else
+void sw_bc_register(const void*, size_t, int) {}
+#endif
 }  // namespace sw
 
 // ---- the context ---------------------------------------------------------------
@@ -245,6 +268,7 @@ int sw_revfft(int m, int n, double* x, const double* trig, const int factors[5])
 int sw_forfft_dev(int m, int n, void* x, int precision, void* stream) {
     return guarded([&] {
         require(m >= 1 && n >= 2 && x, SW_ERR_ARG, "bad forfft arguments");
+        SW_BC_SCOPE(x, (size_t)m * n * (precision == SW_FP64 ? 8 : 4));
         if (precision == SW_FP64) fft1d_dev<double>(m, n, (double*)x, false, (cudaStream_t)stream);
         else fft1d_dev<float>(m, n, (float*)x, false, (cudaStream_t)stream);
         return SW_OK;
@@ -253,6 +277,7 @@ int sw_forfft_dev(int m, int n, void* x, int precision, void* stream) {
 int sw_revfft_dev(int m, int n, void* x, int precision, void* stream) {
     return guarded([&] {
         require(m >= 1 && n >= 2 && x, SW_ERR_ARG, "bad revfft arguments");
+        SW_BC_SCOPE(x, (size_t)m * n * (precision == SW_FP64 ? 8 : 4));
         if (precision == SW_FP64) fft1d_dev<double>(m, n, (double*)x, true, (cudaStream_t)stream);
         else fft1d_dev<float>(m, n, (float*)x, true, (cudaStream_t)stream);
         return SW_OK;
@@ -487,6 +512,8 @@ template <typename T>
 int fft2d_impl(Solver<T>& s, int direction, int nplanes, const void* in, void* out) {
     require(in && out && nplanes >= 1 && (direction == 0 || direction == 1), SW_ERR_ARG, "bad fft2d arguments");
     const int ng = s.ng;
+    SW_BC_SCOPE(in, (size_t)nplanes * ng * ng * sizeof(T));
+    SW_BC_SCOPE(out, (size_t)nplanes * ng * ng * sizeof(T));
     const T* a = (const T*)in;
     T* b = (T*)out;
     if (direction == 0)
@@ -965,6 +992,12 @@ int sw_set_fft_overlap(sw_ctx* ctx, int enable, int* in_use) {
 int sw_set_psolve_toler(sw_ctx* ctx, double toler) {
     return with_solver(ctx, [&](auto& s) {
         s.set_refine_toler(toler);
+        return SW_OK;
+    });
+}
+int sw_set_psolve_relax(sw_ctx* ctx, double omega) {
+    return with_solver(ctx, [&](auto& s) {
+        s.set_psolve_relax(omega);
         return SW_OK;
     });
 }

@@ -88,8 +88,10 @@ struct DevBuf {
         release();
         if (count) SW_CUDA(cudaMalloc(&p, count * sizeof(T)));
         n = count;
+        if (p) sw_bc_register(p, count * sizeof(T), 1);
     }
     void release() {
+        if (p) sw_bc_register(p, 0, 0);
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
@@ -137,17 +139,27 @@ inline void for_planes4(cudaStream_t s, int nplanes, int n2, F f) {
 }
 // Four consecutive elements at p (p 16-byte aligned for float, 32 for double).
 __device__ __forceinline__ void ld4(const float* p, float (&v)[4]) {
+    if (!SW_BC_OK(p, 16, 16)) {
+        v[0] = v[1] = v[2] = v[3] = 0.f;
+        return;
+    }
     const float4 a = *reinterpret_cast<const float4*>(p);
     v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
 }
 __device__ __forceinline__ void ld4(const double* p, double (&v)[4]) {
+    if (!SW_BC_OK(p, 32, 16)) {
+        v[0] = v[1] = v[2] = v[3] = 0.0;
+        return;
+    }
     const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 __device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+    if (!SW_BC_OK(p, 16, 16)) return;
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 __device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+    if (!SW_BC_OK(p, 32, 16)) return;
     reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
     reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
 }

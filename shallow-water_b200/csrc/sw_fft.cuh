@@ -23,6 +23,8 @@
 
 #include <type_traits>
 
+#include "sw_bc.cuh"
+
 namespace sw {
 
 template <typename T> struct C2;
@@ -394,10 +396,12 @@ __device__ __forceinline__ void st_one(const BoundSt<G>& b, int, int col, int k,
 // index as one vector access, and a masked pair store.
 template <typename T>
 __device__ __forceinline__ typename C2<T>::t ldv2(const T* p) {
+    if (!SW_BC_OK(p, 2 * sizeof(T), 2 * sizeof(T))) return typename C2<T>::t{};
     return *reinterpret_cast<const typename C2<T>::t*>(p);
 }
 template <typename T>
 __device__ __forceinline__ typename C2<T>::t ldv2_ro(const T* p) {
+    if (!SW_BC_OK(p, 2 * sizeof(T), 2 * sizeof(T))) return typename C2<T>::t{};
     return __ldg(reinterpret_cast<const typename C2<T>::t*>(p));
 }
 template <typename T>
@@ -409,9 +413,13 @@ __device__ __forceinline__ typename C2<T>::t mk2(T a, T b) {
 }
 template <typename T>
 __device__ __forceinline__ void stv2m(T* p, int m, T a, T b) {
-    if (m == 3) *reinterpret_cast<typename C2<T>::t*>(p) = mk2(a, b);
-    else if (m == 1) p[0] = a;
-    else p[1] = b;
+    if (m == 3) {
+        if (SW_BC_OK(p, 2 * sizeof(T), 2 * sizeof(T))) *reinterpret_cast<typename C2<T>::t*>(p) = mk2(a, b);
+    } else if (m == 1) {
+        if (SW_BC_OK(p, sizeof(T), sizeof(T))) p[0] = a;
+    } else {
+        if (SW_BC_OK(p + 1, sizeof(T), sizeof(T))) p[1] = b;
+    }
 }
 
 template <typename T>

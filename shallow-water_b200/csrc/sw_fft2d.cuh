@@ -45,8 +45,14 @@ template <typename T>
 struct MidPC {
     T* m;
     int ng;
-    __device__ __forceinline__ T operator()(int o, int c, int p) const { return m[((size_t)o * ng + c) * ng + p]; }
-    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { m[((size_t)o * ng + c) * ng + p] = v; }
+    __device__ __forceinline__ T operator()(int o, int c, int p) const {
+        const T* a = m + ((size_t)o * ng + c) * ng + p;
+        return SW_BC_OK(a, sizeof(T), sizeof(T)) ? *a : T(0);
+    }
+    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const {
+        T* a = m + ((size_t)o * ng + c) * ng + p;
+        if (SW_BC_OK(a, sizeof(T), sizeof(T))) *a = v;
+    }
 };
 // intermediate addressed [col + ng*pt] (column index contiguous); columns
 // (c, c+1), c even, are one aligned vector access
@@ -56,16 +62,25 @@ struct MidCP {
     static constexpr bool pair_io = true;
     T* m;
     int ng;
-    __device__ __forceinline__ T operator()(int o, int c, int p) const { return m[((size_t)o * ng + p) * ng + c]; }
-    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { m[((size_t)o * ng + p) * ng + c] = v; }
+    __device__ __forceinline__ T operator()(int o, int c, int p) const {
+        const T* a = m + ((size_t)o * ng + p) * ng + c;
+        return SW_BC_OK(a, sizeof(T), sizeof(T)) ? *a : T(0);
+    }
+    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const {
+        T* a = m + ((size_t)o * ng + p) * ng + c;
+        if (SW_BC_OK(a, sizeof(T), sizeof(T))) *a = v;
+    }
     __device__ __forceinline__ T2 ld2(int o, int c, int p) const {
-        return *reinterpret_cast<const T2*>(m + ((size_t)o * ng + p) * ng + c);
+        const T* a = m + ((size_t)o * ng + p) * ng + c;
+        if (!SW_BC_OK(a, sizeof(T2), sizeof(T2))) return T2{};
+        return *reinterpret_cast<const T2*>(a);
     }
     __device__ __forceinline__ void st2(int o, int c, int p, T a, T b) const {
         T2 v;
         v.x = a;
         v.y = b;
-        *reinterpret_cast<T2*>(m + ((size_t)o * ng + p) * ng + c) = v;
+        T* d = m + ((size_t)o * ng + p) * ng + c;
+        if (SW_BC_OK(d, sizeof(T2), sizeof(T2))) *reinterpret_cast<T2*>(d) = v;
     }
 };
 

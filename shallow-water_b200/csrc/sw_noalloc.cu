@@ -26,6 +26,8 @@
 //     device's current CUDA context; make that first call before any stream capture
 //     that includes this entry point.  A call made under another context of the
 //     device (after a cudaDeviceReset, say) looks the address up again.
+// (compiled without the bounds checks of the debug build: only sw_capi.cu registers memory)
+#undef SW_BOUNDS_CHECK
 #include <cuda.h>
 
 #include <mutex>

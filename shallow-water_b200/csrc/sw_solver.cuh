@@ -50,11 +50,13 @@ struct SweepMidLoad {
     __device__ __forceinline__ T operator()(int o, int c, int p) const {
         T f;
         const T* rw = row(o, p, f);
+        if (!SW_BC_OK(rw + c, sizeof(T), sizeof(T))) return T(0);
         return f * rw[c];
     }
     __device__ __forceinline__ T2 ld2(int o, int c, int p) const {
         T f;
         const T* rw = row(o, p, f);
+        if (!SW_BC_OK(rw + c, sizeof(T2), sizeof(T2))) return T2{};
         T2 v = *reinterpret_cast<const T2*>(rw + c);
         v.x = f * v.x;
         v.y = f * v.y;
@@ -72,12 +74,16 @@ struct SweepPhysStore {
         T* base = kind == 0 ? A : kind == 1 ? B : C;
         return base + ((size_t)((m0 + mm) * L + iz) * ng + p) * ng + c;
     }
-    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const { *dst(o, c, p) = v; }
+    __device__ __forceinline__ void operator()(int o, int c, int p, T v) const {
+        T* d = dst(o, c, p);
+        if (SW_BC_OK(d, sizeof(T), sizeof(T))) *d = v;
+    }
     __device__ __forceinline__ void st2(int o, int c, int p, T a, T b) const {
         T2 v;
         v.x = a;
         v.y = b;
-        *reinterpret_cast<T2*>(dst(o, c, p)) = v;
+        T* d = dst(o, c, p);
+        if (SW_BC_OK(d, sizeof(T2), sizeof(T2))) *reinterpret_cast<T2*>(d) = v;
     }
 };
 
@@ -234,7 +240,8 @@ template <typename T, int NZS, int NV>
 __global__ void __launch_bounds__(THOMAS_THREADS)
 k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __restrict__ SP,
          const double* __restrict__ htdv, const double* __restrict__ etdv, const double* __restrict__ ap,
-         double* __restrict__ PS, double* __restrict__ XF, float* __restrict__ D1, double* __restrict__ part) {
+         double* __restrict__ PS, double* __restrict__ XF, float* __restrict__ D1, float* __restrict__ Cr,
+         double omega, double* __restrict__ part) {
     const int m = blockIdx.y;
     const int i = blockIdx.x * THOMAS_THREADS + threadIdx.x;
     const int nz = NZS ? NZS : nz_rt;
@@ -266,10 +273,13 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
         for (int iz = 0; iz < NZS; iz++) {
             sn += (x[iz] - old[iz]) * (x[iz] - old[iz]);
             sd += old[iz] * old[iz];
-            PS[cb + (size_t)iz * n2] = x[iz];
             if (NV == 3) {
+                PS[cb + (size_t)iz * n2] = x[iz];
                 sx += x[iz] * x[iz];
                 D1[cb + (size_t)iz * n2] = (float)(x[iz] - old[iz]);
+                if (omega != 1.0) Cr[cb + (size_t)iz * n2] = (float)((omega - 1.0) * (x[iz] - old[iz]));
+            } else {
+                PS[cb + (size_t)iz * n2] = omega == 1.0 ? x[iz] : old[iz] + omega * (x[iz] - old[iz]);
             }
         }
         sn += old[NZS] * old[NZS];
@@ -308,10 +318,11 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
             const double old = PS[p];
             sn += (xn - old) * (xn - old);
             sd += old * old;
-            PS[p] = xn;
+            PS[p] = (NV == 3 || omega == 1.0) ? xn : old + omega * (xn - old);
             if (NV == 3) {
                 sx += xn * xn;
                 D1[p] = (float)(xn - old);
+                if (omega != 1.0) Cr[p] = (float)((omega - 1.0) * (xn - old));
             }
         }
 #pragma unroll 4
@@ -321,10 +332,11 @@ k_thomas(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const T* __rest
             const double old = PS[p];
             sn += (xi - old) * (xi - old);
             sd += old * old;
-            PS[p] = xi;
+            PS[p] = (NV == 3 || omega == 1.0) ? xi : old + omega * (xi - old);
             if (NV == 3) {
                 sx += xi * xi;
                 D1[p] = (float)(xi - old);
+                if (omega != 1.0) Cr[p] = (float)((omega - 1.0) * (xi - old));
             }
             xn = xi;
         }
@@ -353,7 +365,7 @@ template <int NZS>
 __global__ void __launch_bounds__(THOMAS_THREADS)
 k_thomas_c(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const float* __restrict__ SP32,
            const double* __restrict__ htdv, const double* __restrict__ etdv, const double* __restrict__ ap,
-           float* __restrict__ Cr, double* __restrict__ XF, double* __restrict__ part) {
+           float* __restrict__ Cr, double omega, double* __restrict__ XF, double* __restrict__ part) {
     const int m = blockIdx.y;
     const int i = blockIdx.x * THOMAS_THREADS + threadIdx.x;
     const int nz = NZS ? NZS : nz_rt;
@@ -382,7 +394,7 @@ k_thomas_c(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const float* 
 #pragma unroll
         for (int iz = 0; iz < NZS; iz++) {
             sn += (x[iz] - old[iz]) * (x[iz] - old[iz]);
-            Cr[cb + (size_t)iz * n2] = (float)x[iz];
+            Cr[cb + (size_t)iz * n2] = (float)(omega == 1.0 ? x[iz] : old[iz] + omega * (x[iz] - old[iz]));
         }
         const int kx = i % ng, ky = i / ng;
         sn *= pweight(kx, ng) * pweight(ky, ng);
@@ -406,7 +418,7 @@ k_thomas_c(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const float* 
             const size_t p = cb + (size_t)(nz - 1) * n2;
             const double old = (double)Cr[p];
             sn += (xn - old) * (xn - old);
-            Cr[p] = (float)xn;
+            Cr[p] = (float)(omega == 1.0 ? xn : old + omega * (xn - old));
         }
 #pragma unroll 4
         for (int iz = nz - 2; iz >= 0; iz--) {
@@ -414,7 +426,7 @@ k_thomas_c(int ng, int nz_rt, int n2, const int* __restrict__ ctl, const float* 
             const double xi = XF[p] + etdv[i + (size_t)n2 * iz] * xn;
             const double old = (double)Cr[p];
             sn += (xi - old) * (xi - old);
-            Cr[p] = (float)xi;
+            Cr[p] = (float)(omega == 1.0 ? xi : old + omega * (xi - old));
             xn = xi;
         }
         const int kx = i % ng, ky = i / ng;
@@ -597,6 +609,10 @@ struct Solver {
     DevBuf<double> eref;       // per member: relative change of the last reference sweep
     DevBuf<double> pnorm;      // per member: weighted |ps|^2 after the last reference sweep
     double refine_toler = 1.0E-7;  // stop rule of the correction sweeps
+    // Relaxation factor of the pressure iteration: each sweep's new iterate is
+    // x + relax (G(x) - x), G one sweep (Thomas solve of the source at x).  1 (the
+    // default) is the reference's iteration (psolve.rs:89-358); set_psolve_relax.
+    double relax = 1.0;
     DevBuf<int> sweep_kind;    // kind of the next sweep: 0 reference (float64), 1 correction (float32)
     cudaStream_t st_if = nullptr;
     int host_kind = 0;         // host-driven loops: kind of the next sweep
@@ -780,6 +796,20 @@ struct Solver {
                 e = nullptr;
             }
         refine_toler = toler;
+    }
+
+    // Relaxation factor of the pressure iteration (see relax).  The iteration's
+    // fixed point does not depend on it; the stop rule measures the unrelaxed change
+    // |G(x) - x|.  The captured step graphs hold the old value, so they are dropped.
+    void set_psolve_relax(double omega) {
+        require(omega > 0.0 && omega <= 1.0, SW_ERR_ARG, "relaxation factor must be in (0, 1]");
+        SW_CUDA(cudaStreamSynchronize(st));
+        for (auto& e : step_exec)
+            if (e) {
+                SW_CUDA(cudaGraphExecDestroy(e));
+                e = nullptr;
+            }
+        relax = omega;
     }
 
     // Planes per 2-D transform launch pair; the captured step graphs hold the old
@@ -2347,15 +2377,33 @@ struct Solver {
                 ld4(SIGY + p, sy);
                 ld4(C2 + p, c2);
                 ld4(C1 + p, c1);
+                if (sizeof(TS) == 4) {  // (a plain if: extended lambdas may not first-capture in if constexpr)
+                    // float32 sweeps: float arithmetic (widening every input to
+                    // float64 made the conversion pipe a limit of this kernel); the
+                    // second difference as (p+ - p) - (p - p-), whose inner
+                    // differences of neighbouring levels are exact
+                    const float hz = (float)hdzi, dzs = (float)dzisq;
 #pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const double dxt = ((double)xp[e] - (double)xm[e]) * hdzi;
-                    const double dyt = ((double)yp[e] - (double)ym[e]) * hdzi;
-                    const double dpdt = ((double)pp[e] - (double)pm[e]) * hdzi;
-                    const double d2 = ((double)pp[e] - 2.0 * (double)pc[e] + (double)pm[e]) * dzisq;
-                    double s = (double)sp0[e] + (double)sx[e] * dxt + (double)sy[e] * dyt;
-                    s += (double)c2[e] * d2 + (double)c1[e] * dpdt;
-                    out[e] = (TS)s;
+                    for (int e = 0; e < 4; e++) {
+                        const float dxt = (float)(xp[e] - xm[e]) * hz;
+                        const float dyt = (float)(yp[e] - ym[e]) * hz;
+                        const float dpdt = (float)(pp[e] - pm[e]) * hz;
+                        const float d2 = (float)((pp[e] - pc[e]) - (pc[e] - pm[e])) * dzs;
+                        float s = (float)sp0[e] + (float)sx[e] * dxt + (float)sy[e] * dyt;
+                        s += (float)c2[e] * d2 + (float)c1[e] * dpdt;
+                        out[e] = (TS)s;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const double dxt = ((double)xp[e] - (double)xm[e]) * hdzi;
+                        const double dyt = ((double)yp[e] - (double)ym[e]) * hdzi;
+                        const double dpdt = ((double)pp[e] - (double)pm[e]) * hdzi;
+                        const double d2 = ((double)pp[e] - 2.0 * (double)pc[e] + (double)pm[e]) * dzisq;
+                        double s = (double)sp0[e] + (double)sx[e] * dxt + (double)sy[e] * dyt;
+                        s += (double)c2[e] * d2 + (double)c1[e] * dpdt;
+                        out[e] = (TS)s;
+                    }
                 }
             } else {
                 // boundary levels: the same stencils, four elements per 16-byte load
@@ -2439,11 +2487,15 @@ struct Solver {
         double* part = red_partial.p;
         const dim3 g(nblk, M);
         float* D1 = refine32 ? R32(9) : nullptr;
-#define SW_THOMAS_CASE(NZV)                                                                                      \
-    if (refine32)                                                                                                \
-        k_thomas<T, NZV, 3><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, D1, part); \
-    else                                                                                                         \
-        k_thomas<T, NZV, 2><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, D1, part);
+        float* Cw = refine32 ? R32(10) : nullptr;
+        const double om = relax;
+#define SW_THOMAS_CASE(NZV)                                                                              \
+    if (refine32)                                                                                        \
+        k_thomas<T, NZV, 3>                                                                              \
+            <<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, D1, Cw, om, part); \
+    else                                                                                                 \
+        k_thomas<T, NZV, 2>                                                                              \
+            <<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SP, htdv, etdv, ap, PS, XF, D1, Cw, om, part);
         switch (nz) {
             case 4: SW_THOMAS_CASE(4) break;
             case 8: SW_THOMAS_CASE(8) break;
@@ -2578,11 +2630,11 @@ struct Solver {
             float* Cw = R32(10);
             double *XF = WD(1), *part = red_partial.p;
             switch (nz) {
-                case 4: k_thomas_c<4><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
-                case 8: k_thomas_c<8><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
-                case 16: k_thomas_c<16><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
-                case 32: k_thomas_c<32><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
-                default: k_thomas_c<0><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, XF, part); break;
+                case 4: k_thomas_c<4><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, relax, XF, part); break;
+                case 8: k_thomas_c<8><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, relax, XF, part); break;
+                case 16: k_thomas_c<16><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, relax, XF, part); break;
+                case 32: k_thomas_c<32><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, relax, XF, part); break;
+                default: k_thomas_c<0><<<g, THOMAS_THREADS, 0, st>>>(ng, nz, n2, ctl, SPC, htdv, etdv, ap, Cw, relax, XF, part); break;
             }
             SW_CHECK_LAUNCH();
             count_launch();

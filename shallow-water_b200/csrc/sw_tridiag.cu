@@ -14,6 +14,8 @@
 // nz + 1 for nz <= 32); c and d are loaded before the recurrences, a and b as
 // the elimination reaches them.  No pivoting: the systems must be safe for Gaussian
 // elimination without it (e.g. diagonally dominant), as the psolve systems are.
+// (compiled without the bounds checks of the debug build: only sw_capi.cu registers memory)
+#undef SW_BOUNDS_CHECK
 #include "sw_core.cuh"
 
 namespace sw {

@@ -92,6 +92,7 @@ pub fn sw_last_error() -> *const c_char;
     pub fn sw_advance(ctx: *mut SwCtx, nsteps: c_int, ggen: c_int) -> c_int;
     pub fn sw_set_graphs(ctx: *mut SwCtx, enable: c_int) -> c_int;
     pub fn sw_set_psolve_toler(ctx: *mut SwCtx, toler: c_double) -> c_int;
+    pub fn sw_set_psolve_relax(ctx: *mut SwCtx, omega: c_double) -> c_int;
     pub fn sw_sweep_counts(ctx: *mut SwCtx, out: *mut c_longlong) -> c_int;
     pub fn sw_set_fft_chunk(ctx: *mut SwCtx, planes: c_int, in_use: *mut c_int) -> c_int;
     pub fn sw_set_fft_single_pass(ctx: *mut SwCtx, enable: c_int, in_use: *mut c_int) -> c_int;

@@ -271,4 +271,10 @@ impl Ensemble {
     pub fn set_psolve_toler(&self, toler: f64) -> anyhow::Result<()> {
         self.ctx.with(|c| check(unsafe { sys::sw_set_psolve_toler(c, toler) }))
     }
+
+    /// Relaxation factor in (0, 1] of the pressure iteration (default 1, the
+    /// reference's iteration); the fixed point does not depend on it.
+    pub fn set_psolve_relax(&self, omega: f64) -> anyhow::Result<()> {
+        self.ctx.with(|c| check(unsafe { sys::sw_set_psolve_relax(c, omega) }))
+    }
 }
