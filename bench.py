@@ -37,7 +37,7 @@ UNIT = "member-steps/s"
 # 102 planes the written planes mostly stay in the 126 MB L2 until after the
 # kernel; at 816 and 1632 planes most of them reach DRAM within it.
 # Keys: (bytes per value of the pass, planes per launch).
-FFT_PASS_DRAM_BYTES = {(4, 102): 26.86e6, (8, 102): 60.4e6,
+FFT_PASS_DRAM_BYTES = {(4, 102): 26.86e6, (8, 102): 60.4e6, (8, 408): 377.3e6,
                        (4, 816): 377.7e6, (4, 1632): 805.9e6,
                        (8, 816): 803.5e6, (8, 1632): 1658.8e6}
 PRECISIONS = ("fp64", "mixed", "fp32")
@@ -376,9 +376,12 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
     member uploads qs, ds, gs, pn from pinned host memory (sw_state_set_all_async),
     advances (sw_advance_async) and downloads qs, ds, gs, pn (sw_state_get_all_async)
     into the same buffers, which the next step uploads, so the run follows one
-    trajectory through host memory; one group's copies overlap the other group's
-    step.  Timed on the host clock from the first copy to the sync that completes
-    the last download."""
+    trajectory through host memory.  The two groups' steps alternate on the device
+    (each step waits for the other group's previous step through an event), so one
+    group's downloads and uploads run while the other group computes; left to the
+    scheduler, the two steps interleave, finish together and leave the device idle
+    while both groups copy.  Timed on the host clock from the first copy to the
+    sync that completes the last download."""
     import torch
     fidx = sw._native.FIELD_INDEX
     half = M // 2
@@ -402,14 +405,26 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
             sw._native.check(L.sw_state_get_all(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), sw._native._dp), n3))
         groups.append((sp, n3, ins, outs))
     dp = sw._native._dp
+    streams = []
+    for sp, _, _, _ in groups:
+        sptr = ctypes.c_void_p()
+        sw._native.check(L.sw_stream(sp.ctx, ctypes.byref(sptr)))
+        streams.append(torch.cuda.ExternalStream(sptr.value))
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    prev = None  # the last queued step's completion event
     for _ in range(steps):
-        for sp, n3, ins, outs in groups:
+        for (sp, n3, ins, outs), stream in zip(groups, streams):
             for k, buf in ins.items():
                 sw._native.check(L.sw_state_set_all_async(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), dp), n3))
+            # the groups' steps alternate: each waits for the other group's step, so
+            # that one group's copies run while the other group computes
+            if prev is not None:
+                stream.wait_event(prev)
             sw._native.check(L.sw_advance_async(sp.ctx, 1, 1))
+            prev = torch.cuda.Event()
+            prev.record(stream)
             for k, buf in outs.items():
                 sw._native.check(L.sw_state_get_all_async(sp.ctx, fidx[k], ctypes.cast(buf.data_ptr(), dp), n3))
     for sp, _, _, _ in groups:
@@ -420,8 +435,8 @@ def e2e_pipelined(sw, L, args, M, prec, local, rank, tune, steps, world, barrier
         g[0].close()
     return {"value": replica_throughput(steps * M, secs, world, "cuda"), "unit": UNIT,
             "h2d_bytes_per_step": 4 * nall * 8, "d2h_bytes_per_step": 4 * nall * 8, "steps": steps,
-            "mode": "two contexts of M/2 members on their own streams; one group's copies overlap the other's "
-                    "step; one sync at the end"}
+            "mode": "two contexts of M/2 members on their own streams; their steps alternate (event-ordered), "
+                    "so one group's copies overlap the other's step; one sync at the end"}
 
 
 def drift(sw, args, rank, local):

@@ -2377,33 +2377,15 @@ struct Solver {
                 ld4(SIGY + p, sy);
                 ld4(C2 + p, c2);
                 ld4(C1 + p, c1);
-                if (sizeof(TS) == 4) {  // (a plain if: extended lambdas may not first-capture in if constexpr)
-                    // float32 sweeps: float arithmetic (widening every input to
-                    // float64 made the conversion pipe a limit of this kernel); the
-                    // second difference as (p+ - p) - (p - p-), whose inner
-                    // differences of neighbouring levels are exact
-                    const float hz = (float)hdzi, dzs = (float)dzisq;
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const float dxt = (float)(xp[e] - xm[e]) * hz;
-                        const float dyt = (float)(yp[e] - ym[e]) * hz;
-                        const float dpdt = (float)(pp[e] - pm[e]) * hz;
-                        const float d2 = (float)((pp[e] - pc[e]) - (pc[e] - pm[e])) * dzs;
-                        float s = (float)sp0[e] + (float)sx[e] * dxt + (float)sy[e] * dyt;
-                        s += (float)c2[e] * d2 + (float)c1[e] * dpdt;
-                        out[e] = (TS)s;
-                    }
-                } else {
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const double dxt = ((double)xp[e] - (double)xm[e]) * hdzi;
-                        const double dyt = ((double)yp[e] - (double)ym[e]) * hdzi;
-                        const double dpdt = ((double)pp[e] - (double)pm[e]) * hdzi;
-                        const double d2 = ((double)pp[e] - 2.0 * (double)pc[e] + (double)pm[e]) * dzisq;
-                        double s = (double)sp0[e] + (double)sx[e] * dxt + (double)sy[e] * dyt;
-                        s += (double)c2[e] * d2 + (double)c1[e] * dpdt;
-                        out[e] = (TS)s;
-                    }
+                for (int e = 0; e < 4; e++) {
+                    const double dxt = ((double)xp[e] - (double)xm[e]) * hdzi;
+                    const double dyt = ((double)yp[e] - (double)ym[e]) * hdzi;
+                    const double dpdt = ((double)pp[e] - (double)pm[e]) * hdzi;
+                    const double d2 = ((double)pp[e] - 2.0 * (double)pc[e] + (double)pm[e]) * dzisq;
+                    double s = (double)sp0[e] + (double)sx[e] * dxt + (double)sy[e] * dyt;
+                    s += (double)c2[e] * d2 + (double)c1[e] * dpdt;
+                    out[e] = (TS)s;
                 }
             } else {
                 // boundary levels: the same stencils, four elements per 16-byte load

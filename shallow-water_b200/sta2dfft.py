@@ -30,8 +30,20 @@ class D2FFT:
     def spctop(self, svar, rvar):
         return self._sp.spctop(svar, rvar)
 
+    def _check_k(self, rk, own, axis):
+        # The GPU derivative multiplies by the integer wavenumber of each mode, which
+        # is the reference's rk array (pi / l) * k on the 2 pi domain; another array
+        # would silently give another derivative, so it is refused.
+        rk = np.asarray(rk, dtype=np.float64).ravel()
+        if rk.shape != own.shape or np.abs(rk - own).max() > 1e-12 * np.abs(own).max():
+            raise ValueError("D2FFT.%sderiv: only the domain's own wavenumbers (D2FFT.k%s) are supported" % (axis, axis))
+
     def xderiv(self, rkx, var, der):
+        """x derivative of a spectral field (src/sta2dfft.rs:128-152)."""
+        self._check_k(rkx, self.kx, "x")
         return self._sp.xderiv(var, der)
 
     def yderiv(self, rky, var, der):
+        """y derivative of a spectral field (src/sta2dfft.rs:157-184)."""
+        self._check_k(rky, self.ky, "y")
         return self._sp.yderiv(var, der)

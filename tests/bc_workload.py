@@ -60,7 +60,9 @@ def run(sw):
     energies, spec, f3, f2 = sw.nhswps.savegrid_data(st)
     out["ng48_gs"] = _get(sw, sp, 0, "gs")
     out["ng48_energies"] = np.asarray(energies, dtype=np.float64)
-    out["ng48_f3"] = np.asarray(f3, dtype=np.float64).ravel()
+    out["ng48_spectra"] = np.asarray(spec, dtype=np.float64).ravel()
+    out["ng48_f3"] = np.concatenate([np.asarray(f3[k], dtype=np.float64) for k in sorted(f3)])
+    out["ng48_f2"] = np.concatenate([np.asarray(f2[k], dtype=np.float64) for k in sorted(f2)])
     sp.close()
     # batched 2-D transforms on caller buffers (n = 96 generic, n = 256 register-staged)
     for ng in (96, 256):

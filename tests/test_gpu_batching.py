@@ -261,7 +261,12 @@ def test_ten_steps_256_all_precisions_vs_oracle(sw, oracle):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_uneven_ensemble_members_match_single_runs(sw, precision):
     """sw_ensemble: members of uneven grids (three (ng, nz) groups) advanced by one
-    graph launch per step of every member match their single runs at 1e-12."""
+    graph launch per step of every member match their single runs: at 1e-12 in
+    FP64.  In SW_MIXED the choice between a float64 and a float32 sweep is made per
+    context from all its members, so a member in a group can take a different
+    sweep schedule than alone; its iterates then differ by float32 rounding
+    relative to the small corrections, far below the 1e-7 stop rule (measured
+    2e-12), and the bound is 1e-9."""
     prec = _prec(sw, precision)
     draws = [(32, 4), (48, 8), (32, 4), (64, 4), (48, 8)]
     ens = sw.nhswps.Ensemble([d[0] for d in draws], [d[1] for d in draws], precision=prec)
@@ -280,9 +285,10 @@ def test_uneven_ensemble_members_match_single_runs(sw, precision):
         sp = sw.Spectral(ng, nz, precision=prec)
         st = sw.nhswps.initial_state(sp, z[k], np.zeros_like(z[k]), np.zeros_like(z[k]))
         sw._native.check(sw._native.lib().sw_advance(sp.ctx, 3, 1))
+        tol = 1e-12 if precision == "fp64" else 1e-9
         for f in ("qs", "ds", "gs", "pn"):
             err = rel_l2(got[k][f], st.get(f))
-            assert err <= 1e-12, "member %d %s rel-L2 %.3e" % (k, f, err)
+            assert err <= tol, "member %d %s rel-L2 %.3e" % (k, f, err)
         sp.close()
 
 

@@ -446,3 +446,27 @@ def test_nhswps_end_to_end(sw, tmp_path, ng, nz, dt, tsim):
     ref = g["%d_%d/2d/q.r4" % (ng, nz)]
     got = np.fromfile(tmp_path / "2d/q.r4", dtype="<f4")
     assert np.abs(got - ref).max() <= 2e-5 * max(1.0, np.abs(ref).max())
+
+
+def test_d2fft_class_golden(sw):
+    """sta2dfft's D2FFT (src/sta2dfft.rs:37-184) through the package's class: its
+    trig tables equal initfft's, ptospc / spctop and the derivatives with the
+    domain's own wavenumbers equal the reference's golden outputs, and a foreign
+    wavenumber array is refused rather than ignored."""
+    g = golden("sta2dfft")
+    d = sw.sta2dfft.D2FFT(32, 32)
+    f, trig = sw.stafft.initfft(32)
+    assert np.array_equal(d.xtrig, trig) and list(d.xfactors) == list(f)
+    s = np.zeros(32 * 32)
+    _rel(d.ptospc(g["ptospc/ptospc_ng32_rvar.bin"], s), g["ptospc/ptospc_ng32_svar2.bin"])
+    r = np.zeros(32 * 32)
+    _rel(d.spctop(g["spctop/spctop_ng32_svar.bin"], r), g["spctop/spctop_ng32_rvar2.bin"])
+    for which, case, ng in (("x", 1, 32), ("x", 2, 24), ("y", 1, 32), ("y", 2, 24)):
+        dd = d if ng == 32 else sw.sta2dfft.D2FFT(ng, ng)
+        var = g["deriv/%sderiv_%d_var.bin" % (which, case)]
+        rk = g["deriv/%sderiv_%d_rk%s.bin" % (which, case, which)]
+        out = np.zeros(ng * ng)
+        (dd.xderiv if which == "x" else dd.yderiv)(rk, var, out)
+        _close(out, g["deriv/%sderiv_%d_der2.bin" % (which, case)], 0.0)
+    with pytest.raises(ValueError):
+        d.xderiv(2.0 * d.kx, g["deriv/xderiv_1_var.bin"], np.zeros(32 * 32))
