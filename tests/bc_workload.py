@@ -51,6 +51,34 @@ def run(sw):
         for k in ("qs", "ds", "gs", "pn"):
             out["%s_%s" % (name, k)] = _get(sw, sp, 1, k)
         sp.close()
+    # the reference's one-function-at-a-time entry points (their own kernels, not
+    # the fused step's), on a float64 and a float32 context
+    for name, prec in (("fn64", sw.SW_FP64), ("fn32", sw.SW_FP32)):
+        sp = _ensemble(sw, 32, 4, 1, prec, 11)
+        st = sw.State(sp, member=0)
+        sw.nhswps.vertical(st)
+        sig = sw.nhswps.coeffs(st)
+        sp0 = sw.nhswps.cpsource(st)
+        sw.nhswps.psolve(st)
+        src = sw.nhswps.source(st)
+        out["%s_sigx" % name] = sig[0]
+        out["%s_sp0" % name] = sp0
+        out["%s_sgs" % name] = src[2]
+        out["%s_pn" % name] = _get(sw, sp, 0, "pn")
+        sp.close()
+    # an uneven ensemble: two (ng, nz) groups advanced by one graph launch per step
+    draws = [(32, 4), (48, 4), (32, 4)]
+    ens = sw.nhswps.Ensemble([d[0] for d in draws], [d[1] for d in draws], precision=sw.SW_MIXED)
+    for k, (ng, nz) in enumerate(draws):
+        qq = sw.vstrip.pv_strip(ng)
+        rng = np.random.default_rng(300 + k)
+        q3 = np.tile(qq, nz + 1) + rng.normal(0.0, 1.0e-3, ng * ng * (nz + 1))
+        ens.initial_state(k, q3, np.zeros_like(q3), np.zeros_like(q3))
+    ens.invert_all()
+    ens.advance(2)
+    for k in range(len(draws)):
+        out["mixed_ens%d_gs" % k] = ens.state(k).get("gs").ravel(order="F")
+    ens.close()
     # a length served by the generic tile pass, and the savegrid outputs
     sp = _ensemble(sw, 48, 8, 1, sw.SW_FP64, 3)
     sw._native.check(L.sw_advance(sp.ctx, 1, 1))
