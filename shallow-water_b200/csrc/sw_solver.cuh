@@ -717,10 +717,10 @@ struct Solver {
             SW_CUDA(cudaMemset(pnorm.p, 0, sizeof(double) * M));
             sweep_kind.alloc(1);
             SW_CUDA(cudaMemset(sweep_kind.p, 0, sizeof(int)));
-            xh.alloc(3 * nf);
-            SW_CUDA(cudaMemset(xh.p, 0, sizeof(double) * 3 * nf));
-            xflag.alloc(3);
-            SW_CUDA(cudaMemset(xflag.p, 0, 3 * sizeof(int)));
+            xh.alloc(6 * nf);
+            SW_CUDA(cudaMemset(xh.p, 0, sizeof(double) * 6 * nf));
+            xflag.alloc(6);
+            SW_CUDA(cudaMemset(xflag.p, 0, 6 * sizeof(int)));
             SW_CUDA(cudaStreamSynchronize(st));
             for (auto& e : step_exec)
                 if (e) {
@@ -734,54 +734,72 @@ struct Solver {
     }
 
     // Mixed path: the first iterate of each pressure solve of a step is predicted
-    // from the previous step, where the reference starts from the previous solve's
+    // from the previous steps, where the reference starts from the previous solve's
     // solution.  A step solves three times, in slots j = 0 (at the step's start, the
     // ggen solve), 1 (after the predictor) and 2 (after the corrector).  At the start
     // of slot j of step n, ps holds the solution of the solve before it (slot j - 1
-    // of step n, or slot 2 of step n - 1), and the first iterate is that plus the
-    // change between the same two slots one step earlier:
-    //   ps <- ps + (H[j] - H[j-1])     H[j] = solution of slot j in step n - 1
-    // then H[j-1] <- the old ps.  The iteration and its fixed point are unchanged;
-    // a nearer first iterate needs fewer sweeps.  A member whose predicted change is
-    // larger than ps itself (|H[j] - H[j-1]| > |ps|: a history from another run), or
-    // whose history is not yet written, keeps ps.  Steps without the ggen solve
-    // clear the history.
+    // of step n, or slot 2 of step n - 1).  With D1 and D2 the changes between the
+    // same two slots one and two steps earlier, the first iterate is
+    //   ps + 2 D1 - D2     (the change extrapolated linearly over the steps), or
+    //   ps + D1            (while only one earlier step is recorded, or when the
+    //                       extrapolation's correction |D1 - D2| exceeds |D1|).
+    // H[j] (xh slots 0..2) holds the solution of slot j one step earlier and G[j]
+    // (slots 3..5) two steps earlier; then G[j-1] <- H[j-1], H[j-1] <- the old ps.
+    // The iteration and its fixed point are unchanged; a nearer first iterate needs
+    // fewer sweeps.  A member whose predicted change is larger than ps itself
+    // (|D1| > |ps|: a history from another run), or whose history is not yet
+    // written, keeps ps.  Steps without the ggen solve clear the history.
     void extrapolate_guess(int j) {
         const int n2 = this->n2, L = this->L, ML = this->ML, M = this->M;
         const int jp = (j + 2) % 3;
         const long long nm = (long long)L * n2;
         double* PS = ps;
         double *Hj = xh.p + (size_t)j * nf, *Hp = xh.p + (size_t)jp * nf;
+        double *Gj = xh.p + (size_t)(3 + j) * nf, *Gp = xh.p + (size_t)(3 + jp) * nf;
         int* fl = xflag.p;
-        double* sums = red_out.p + (size_t)6 * ML;  // 2 M values (red_out holds 8 ML + 64)
-        reduce_groups<2>(st, M, nm, 0u,
+        double* sums = red_out.p + (size_t)6 * ML;  // 3 M values (red_out holds 8 ML + 64)
+        reduce_groups<3>(st, M, nm, 0u,
             [=] __device__(int g, long long i) {
                 const size_t p = (size_t)g * nm + i;
-                const double d = Hj[p] - Hp[p];
-                RedVals<2> rv;
-                rv.v[0] = d * d;
+                const double d1 = Hj[p] - Hp[p];
+                const double d2 = Gj[p] - Gp[p];
+                RedVals<3> rv;
+                rv.v[0] = d1 * d1;
                 rv.v[1] = PS[p] * PS[p];
+                rv.v[2] = (d1 - d2) * (d1 - d2);
                 return rv;
             }, red_partial.p, sums);
         for_planes4(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L;
             const size_t p = (size_t)q * n2 + i;
-            double c[4];
+            double c[4], a[4], b[4];
             ld4(PS + p, c);
-            if (fl[j] && fl[jp] && sums[2 * m] <= sums[2 * m + 1]) {
-                double a[4], b[4], o[4];
+            ld4(Hp + p, b);
+            if (fl[j] && fl[jp] && sums[3 * m] <= sums[3 * m + 1]) {
+                double o[4];
                 ld4(Hj + p, a);
-                ld4(Hp + p, b);
+                if (fl[3 + j] && fl[3 + jp] && sums[3 * m + 2] <= sums[3 * m]) {
+                    double ga[4], gb[4];
+                    ld4(Gj + p, ga);
+                    ld4(Gp + p, gb);
 #pragma unroll
-                for (int e = 0; e < 4; e++) o[e] = c[e] + (a[e] - b[e]);
+                    for (int e = 0; e < 4; e++) o[e] = c[e] + (2.0 * (a[e] - b[e]) - (ga[e] - gb[e]));
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) o[e] = c[e] + (a[e] - b[e]);
+                }
                 st4(PS + p, o);
             }
+            st4(Gp + p, b);
             st4(Hp + p, c);
         });
-        for_cols(st, 1, [=] __device__(int) { fl[jp] = 1; });
+        for_cols(st, 1, [=] __device__(int) {
+            fl[3 + jp] = fl[jp];
+            fl[jp] = 1;
+        });
     }
     void reset_guess_history() {
-        if (xflag.p) SW_CUDA(cudaMemsetAsync(xflag.p, 0, 3 * sizeof(int), st));
+        if (xflag.p) SW_CUDA(cudaMemsetAsync(xflag.p, 0, 6 * sizeof(int), st));
     }
 
     // Stop rule of the correction sweeps (the mixed path); the captured step graphs

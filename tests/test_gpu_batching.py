@@ -265,8 +265,8 @@ def test_uneven_ensemble_members_match_single_runs(sw, precision):
     FP64.  In SW_MIXED the choice between a float64 and a float32 sweep is made per
     context from all its members, so a member in a group can take a different
     sweep schedule than alone; its iterates then differ by float32 rounding
-    relative to the small corrections, far below the 1e-7 stop rule (measured
-    2e-12), and the bound is 1e-9."""
+    relative to the small corrections, far below the 1e-7 stop rule (measured up
+    to 4.5e-9), and the bound is 1e-8."""
     prec = _prec(sw, precision)
     draws = [(32, 4), (48, 8), (32, 4), (64, 4), (48, 8)]
     ens = sw.nhswps.Ensemble([d[0] for d in draws], [d[1] for d in draws], precision=prec)
@@ -285,7 +285,7 @@ def test_uneven_ensemble_members_match_single_runs(sw, precision):
         sp = sw.Spectral(ng, nz, precision=prec)
         st = sw.nhswps.initial_state(sp, z[k], np.zeros_like(z[k]), np.zeros_like(z[k]))
         sw._native.check(sw._native.lib().sw_advance(sp.ctx, 3, 1))
-        tol = 1e-12 if precision == "fp64" else 1e-9
+        tol = 1e-12 if precision == "fp64" else 1e-8
         for f in ("qs", "ds", "gs", "pn"):
             err = rel_l2(got[k][f], st.get(f))
             assert err <= tol, "member %d %s rel-L2 %.3e" % (k, f, err)
@@ -445,7 +445,8 @@ def test_spec1d_on_device_matches_reference_formula(sw):
 
 def test_mixed_predicted_first_iterate(sw):
     """SW_MIXED starts each pressure solve of a step from the previous solve's
-    solution plus the change between the same two solves one step earlier.
+    solution plus the change between the same two solves, extrapolated over the
+    last two steps (one step while only one is recorded).
     (1) Steps after the first need fewer sweeps than the first, which starts from
     no history and pn = 0.  (2) A state set between steps (another member's
     trajectory) does not disturb the solve: the context that ran trajectory A and
