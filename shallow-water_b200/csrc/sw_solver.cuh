@@ -717,10 +717,10 @@ struct Solver {
             SW_CUDA(cudaMemset(pnorm.p, 0, sizeof(double) * M));
             sweep_kind.alloc(1);
             SW_CUDA(cudaMemset(sweep_kind.p, 0, sizeof(int)));
-            xh.alloc(6 * nf);
-            SW_CUDA(cudaMemset(xh.p, 0, sizeof(double) * 6 * nf));
-            xflag.alloc(6);
-            SW_CUDA(cudaMemset(xflag.p, 0, 6 * sizeof(int)));
+            xh.alloc(9 * nf);
+            SW_CUDA(cudaMemset(xh.p, 0, sizeof(double) * 9 * nf));
+            xflag.alloc(9);
+            SW_CUDA(cudaMemset(xflag.p, 0, 9 * sizeof(int)));
             SW_CUDA(cudaStreamSynchronize(st));
             for (auto& e : step_exec)
                 if (e) {
@@ -738,13 +738,14 @@ struct Solver {
     // solution.  A step solves three times, in slots j = 0 (at the step's start, the
     // ggen solve), 1 (after the predictor) and 2 (after the corrector).  At the start
     // of slot j of step n, ps holds the solution of the solve before it (slot j - 1
-    // of step n, or slot 2 of step n - 1).  With D1 and D2 the changes between the
-    // same two slots one and two steps earlier, the first iterate is
-    //   ps + 2 D1 - D2     (the change extrapolated linearly over the steps), or
-    //   ps + D1            (while only one earlier step is recorded, or when the
-    //                       extrapolation's correction |D1 - D2| exceeds |D1|).
-    // H[j] (xh slots 0..2) holds the solution of slot j one step earlier and G[j]
-    // (slots 3..5) two steps earlier; then G[j-1] <- H[j-1], H[j-1] <- the old ps.
+    // of step n, or slot 2 of step n - 1).  With D1, D2, D3 the changes between the
+    // same two slots one, two and three steps earlier, the change is extrapolated
+    // over the steps by a polynomial of degree 0, 1 or 2:
+    //   ps + D1,   ps + 2 D1 - D2,   ps + 3 D1 - 3 D2 + D3,
+    // the highest degree whose history is recorded and whose added term is smaller
+    // than the one before it (|D1 - D2| <= |D1|, |D1 - 2 D2 + D3| <= |D1 - D2|).
+    // H[j], G[j], K[j] (xh slots 0..2, 3..5, 6..8) hold the solution of slot j one,
+    // two and three steps earlier; then K[j-1] <- G[j-1] <- H[j-1] <- the old ps.
     // The iteration and its fixed point are unchanged; a nearer first iterate needs
     // fewer sweeps.  A member whose predicted change is larger than ps itself
     // (|D1| > |ps|: a history from another run), or whose history is not yet
@@ -756,50 +757,68 @@ struct Solver {
         double* PS = ps;
         double *Hj = xh.p + (size_t)j * nf, *Hp = xh.p + (size_t)jp * nf;
         double *Gj = xh.p + (size_t)(3 + j) * nf, *Gp = xh.p + (size_t)(3 + jp) * nf;
+        double *Kj = xh.p + (size_t)(6 + j) * nf, *Kp = xh.p + (size_t)(6 + jp) * nf;
         int* fl = xflag.p;
-        double* sums = red_out.p + (size_t)6 * ML;  // 3 M values (red_out holds 8 ML + 64)
-        reduce_groups<3>(st, M, nm, 0u,
+        double* sums = red_out.p + (size_t)6 * ML;  // 4 M values (red_out holds 8 ML + 64)
+        reduce_groups<4>(st, M, nm, 0u,
             [=] __device__(int g, long long i) {
                 const size_t p = (size_t)g * nm + i;
                 const double d1 = Hj[p] - Hp[p];
                 const double d2 = Gj[p] - Gp[p];
-                RedVals<3> rv;
+                const double d3 = Kj[p] - Kp[p];
+                RedVals<4> rv;
                 rv.v[0] = d1 * d1;
                 rv.v[1] = PS[p] * PS[p];
                 rv.v[2] = (d1 - d2) * (d1 - d2);
+                rv.v[3] = (d1 - 2.0 * d2 + d3) * (d1 - 2.0 * d2 + d3);
                 return rv;
             }, red_partial.p, sums);
         for_planes4(st, ML, n2, [=] __device__(int q, int i) {
             const int m = q / L;
             const size_t p = (size_t)q * n2 + i;
-            double c[4], a[4], b[4];
+            double c[4], hb[4], gb[4];
             ld4(PS + p, c);
-            ld4(Hp + p, b);
-            if (fl[j] && fl[jp] && sums[3 * m] <= sums[3 * m + 1]) {
-                double o[4];
-                ld4(Hj + p, a);
-                if (fl[3 + j] && fl[3 + jp] && sums[3 * m + 2] <= sums[3 * m]) {
-                    double ga[4], gb[4];
-                    ld4(Gj + p, ga);
-                    ld4(Gp + p, gb);
+            ld4(Hp + p, hb);
+            ld4(Gp + p, gb);
+            const double* sm = sums + 4 * m;
+            const int deg = !(fl[j] && fl[jp] && sm[0] <= sm[1]) ? -1
+                            : !(fl[3 + j] && fl[3 + jp] && sm[2] <= sm[0]) ? 0
+                            : !(fl[6 + j] && fl[6 + jp] && sm[3] <= sm[2]) ? 1 : 2;
+            if (deg >= 0) {
+                double o[4], ha[4];
+                ld4(Hj + p, ha);
+                if (deg == 0) {
 #pragma unroll
-                    for (int e = 0; e < 4; e++) o[e] = c[e] + (2.0 * (a[e] - b[e]) - (ga[e] - gb[e]));
+                    for (int e = 0; e < 4; e++) o[e] = c[e] + (ha[e] - hb[e]);
                 } else {
+                    double ga[4];
+                    ld4(Gj + p, ga);
+                    if (deg == 1) {
 #pragma unroll
-                    for (int e = 0; e < 4; e++) o[e] = c[e] + (a[e] - b[e]);
+                        for (int e = 0; e < 4; e++) o[e] = c[e] + (2.0 * (ha[e] - hb[e]) - (ga[e] - gb[e]));
+                    } else {
+                        double ka[4], kb[4];
+                        ld4(Kj + p, ka);
+                        ld4(Kp + p, kb);
+#pragma unroll
+                        for (int e = 0; e < 4; e++)
+                            o[e] = c[e] + (3.0 * (ha[e] - hb[e]) - 3.0 * (ga[e] - gb[e]) + (ka[e] - kb[e]));
+                    }
                 }
                 st4(PS + p, o);
             }
-            st4(Gp + p, b);
+            st4(Kp + p, gb);
+            st4(Gp + p, hb);
             st4(Hp + p, c);
         });
         for_cols(st, 1, [=] __device__(int) {
+            fl[6 + jp] = fl[3 + jp];
             fl[3 + jp] = fl[jp];
             fl[jp] = 1;
         });
     }
     void reset_guess_history() {
-        if (xflag.p) SW_CUDA(cudaMemsetAsync(xflag.p, 0, 6 * sizeof(int), st));
+        if (xflag.p) SW_CUDA(cudaMemsetAsync(xflag.p, 0, 9 * sizeof(int), st));
     }
 
     // Stop rule of the correction sweeps (the mixed path); the captured step graphs

@@ -445,8 +445,8 @@ def test_spec1d_on_device_matches_reference_formula(sw):
 
 def test_mixed_predicted_first_iterate(sw):
     """SW_MIXED starts each pressure solve of a step from the previous solve's
-    solution plus the change between the same two solves, extrapolated over the
-    last two steps (one step while only one is recorded).
+    solution plus the change between the same two solves, extrapolated over up to
+    three earlier steps (fewer while fewer are recorded).
     (1) Steps after the first need fewer sweeps than the first, which starts from
     no history and pn = 0.  (2) A state set between steps (another member's
     trajectory) does not disturb the solve: the context that ran trajectory A and
