@@ -860,7 +860,11 @@ struct Solver {
                 SW_CUDA(cudaGraphExecDestroy(e));
                 e = nullptr;
             }
-        return fft.set_chunk(planes);
+        const int c = fft.set_chunk(planes);
+        if constexpr (sizeof(T) == 8) {
+            if (refine32) f32.set_chunk(2 * c);  // the float32 engine: the same bytes per chunk
+        }
+        return c;
     }
 
     // Single-pass cluster transforms at n = 256 on or off (off by default); like the
@@ -889,7 +893,14 @@ struct Solver {
                 SW_CUDA(cudaGraphExecDestroy(e));
                 e = nullptr;
             }
-        return fft.set_overlap(enable != 0);
+        const bool on = fft.set_overlap(enable != 0);
+        if constexpr (sizeof(T) == 8) {
+            if (refine32) {
+                f32.set_overlap(on);
+                f32.set_chunk(2 * fft.chunk);
+            }
+        }
+        return on;
     }
 
     // Columns per tile of the n = 256 tile passes (16 or 32); like the chunk, the
